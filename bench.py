@@ -1,0 +1,388 @@
+"""Benchmark of the per-step lattice update on the flow-past-sphere workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--config 1|2]
+                    [--storage f32|f16|bf16]
+
+Workload (default): 512x256x256 FP32 D3Q27 grid with one 2:1 refinement level over a
+128x96x96 coarse block (256x192x192 fine cells), sphere D=48 at (128,128,128), Re=1e5,
+cumulant collision + Smagorinsky C_s=0.1, free-slip walls, velocity inlet, pressure
+outlet.  One step = one coarse time step = updateGrid(grids, 0): coarse streaming +
+update, two fine streaming + update, one coarse/fine transfer: 50,843,696 cell updates.
+Inputs (4.64 GB coarse + 1.02 GB fine) are larger than L2, so no L2 flush is needed.
+
+Prints ONE JSON line (rank 0).  `value` is MLUPS over the device-timed region (CUDA events,
+max over ranks); `e2e` is the same metric through the public API with host buffers: the
+state is uploaded from pinned host memory, every step reads the FP64 drag back to the host
+(as the reference driver does), and the final state is downloaded.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "D3Q27 MLUPS & % HBM roofline: FP32 plain vs FP16-store+learned SGS, same err"
+BYTES_PER_UPDATE = {"f32": 216, "f16": 108, "bf16": 108}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="native", choices=["native", "reference"])
+    p.add_argument("--config", type=int, default=2, choices=[1, 2])
+    p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-sample-steps", type=int, default=2)
+    return p.parse_args()
+
+
+def workload(args):
+    from periodicshiftlbm_b200.cases import config1, config2
+
+    return config2() if args.config == 2 else config1()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+# ------------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ------------------------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(REPO, "gpurun_out", f"clocks_rank{gpu_index}.csv") if os.path.isdir(
+            os.path.join(REPO, "gpurun_out")) else f"/tmp/psl_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[4:]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        loaded = [r for r in rows if r[0] > 0.5 * r[1]] or rows
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in loaded for i in range(1, 5) if "Active" in r[2][i]})
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------------------------
+# measured peaks and the ncu traffic summary
+# ------------------------------------------------------------------------------------------
+def hbm_peak():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str, storage: str):
+    """dram bytes read+written per launch of the coarse step kernel from the committed ncu
+    summary (profiles/step_kernel_<storage>_sphere512.md), or None."""
+    path = os.path.join(REPO, "profiles", f"step_kernel_{storage}_sphere512.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+# ------------------------------------------------------------------------------------------
+# native (CUDA) arm
+# ------------------------------------------------------------------------------------------
+def run_native(args):
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from periodicshiftlbm_b200 import (
+        applyCoarseFineGridCommunication,
+        applyLocalCellUpdate,
+        applyStreaming,
+        getSphereForce,
+    )
+    from periodicshiftlbm_b200.cases import make_sphere_grids
+
+    cfg = workload(args)
+    stream = torch.cuda.Stream()
+    grids, case = make_sphere_grids(cfg, storage=args.storage)
+    for g in grids:
+        g.set_stream(stream.cuda_stream)
+    torch.cuda.synchronize()
+    levels = len(grids)
+    ev = {"coarse": [], "fine": []}
+
+    def update(level, record):
+        """updateGrid (flowAroundSphereMainSingle.cu:158-167) with events around the
+        update launches when `record`."""
+        g = grids[level]
+        applyStreaming(g)
+        if record:
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            applyLocalCellUpdate(g)
+            b.record(stream)
+            ev["coarse" if level == 0 else "fine"].append((a, b))
+        else:
+            applyLocalCellUpdate(g)
+        if level < levels - 1:
+            update(level + 1, record)
+            update(level + 1, record)
+            applyCoarseFineGridCommunication(g, grids[level + 1])
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        update(0, False)
+    torch.cuda.synchronize()
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        update(0, True)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier()
+    ms = t0.elapsed_time(t1)
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    updates = cfg.updates_per_step()
+    value = updates * args.steps * world / (ms * 1e-3) / 1e6
+
+    # roofline of the dominant kernel: the coarse-grid update
+    coarse_ms = statistics.mean(a.elapsed_time(b) for a, b in ev["coarse"])
+    fine_ms = statistics.mean(a.elapsed_time(b) for a, b in ev["fine"]) if ev["fine"] else None
+    info0 = cfg.infos()[0]
+    coarse_updates = info0.cellCount
+    if cfg.refine:
+        (i0, j0, k0), (i1, j1, k1) = cfg.refine
+        coarse_updates -= (i1 - i0 - 4) * (j1 - j0 - 4) * (k1 - k0 - 4)
+    bpu = BYTES_PER_UPDATE[args.storage]
+    coarse_bytes = bpu * coarse_updates
+    peak, peak_kind = hbm_peak()
+    achieved = coarse_bytes / (coarse_ms * 1e-3) / 1e9
+
+    # ---- end to end through the public API with host buffers ----
+    host_state = [np.ascontiguousarray(g.fArray) for g in grids]
+    pinned = [torch.from_numpy(h).pin_memory() for h in host_state]
+    torch.cuda.synchronize()
+    barrier()
+    e0 = time.perf_counter()
+    for g, h in zip(grids, pinned):
+        g.fArray = h.numpy()
+    drags = []
+    for _ in range(args.steps):
+        update(0, False)
+        drags.append(float(getSphereForce(grids[-1], case)[0]))
+    out_state = [g.fArray for g in grids]
+    torch.cuda.synchronize()
+    e_s = time.perf_counter() - e0
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_s = float(t.item())
+    state_bytes = sum(h.nbytes for h in host_state)
+    e2e_value = updates * args.steps * world / e_s / 1e6
+
+    line = {
+        "metric": METRIC,
+        "value": round(value, 1),
+        "unit": "MLUPS",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32" if args.storage == "f32" else f"{args.storage}-storage/f32-math",
+        "data": "synthetic",
+        "config": {
+            "workload": cfg.name,
+            "grid": [cfg.nx, cfg.ny, cfg.nz],
+            "refine_block": cfg.refine,
+            "storage": args.storage,
+            "updates_per_step": updates,
+            "reference_formula_updates_per_step": cfg.reference_updates_per_step(),
+            "collision": "cumulant + Smagorinsky" if cfg.smagorinsky else "cumulant",
+            "l2": "inputs larger than L2 (no flush)" if cfg.refine else "state fits partly in L2",
+            "parallelism": f"replicas x{world}",
+        },
+        "roofline": {
+            "bound": "hbm",
+            "kernel": "step_kernel (coarse grid)",
+            "achieved": round(achieved, 1),
+            "peak": peak,
+            "peak_kind": peak_kind,
+            "unit": "GB/s",
+            "frac": round(achieved / peak, 4),
+            "traffic": ncu_traffic("step_kernel", args.storage),
+            "algorithmic_bytes_per_launch": coarse_bytes,
+            "launch_ms": round(coarse_ms, 4),
+            "fine_launch_ms": round(fine_ms, 4) if fine_ms else None,
+        },
+        "e2e": {
+            "value": round(e2e_value, 1),
+            "unit": "MLUPS",
+            "h2d_bytes_per_step": round(state_bytes / args.steps),
+            "d2h_bytes_per_step": round(state_bytes / args.steps) + 24,
+            "note": "state uploaded once and downloaded once per run, drag read back every step",
+        },
+        "gpu_launches": args.steps * (1 + 2 * (levels - 1) + (levels - 1)) if levels > 1 else args.steps,
+        "clocks": clocks,
+        "drag_last": drags[-1] if drags else None,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cfg, args.cpu_sample_steps)
+    for g in grids:
+        g.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------
+# the reference's own CPU code (oracle/_ref, compiled for the host): CPU baseline / arm
+# ------------------------------------------------------------------------------------------
+def _ref_case(cfg):
+    from oracle.bindings import SphereCase as RefCase
+
+    return RefCase(nx=cfg.nx, ny=cfg.ny, nz=cfg.nz, sphere=tuple(cfg.sphere), radius=cfg.radius, u_in=cfg.u_in,
+                   nu=cfg.nu, smagorinsky=cfg.smagorinsky, wall_mode=cfg.wall_mode, seed=cfg.seed, noise=cfg.noise,
+                   refine=cfg.refine)
+
+
+def _ref_lib():
+    from oracle.bindings import RefLib, ref_available
+
+    if ref_available():
+        return RefLib(), "reference"
+    from oracle.bindings import OracleLib
+
+    return OracleLib(), "port"
+
+
+def cpu_baseline(cfg, sample_steps):
+    lib, kind = _ref_lib()
+    sim = lib.sim(_ref_case(cfg))
+    t = time.perf_counter()
+    sim.run(sample_steps)
+    dt = time.perf_counter() - t
+    value = cfg.updates_per_step() * sample_steps / dt / 1e6
+    sim.close()
+    return {"value": round(value, 2), "unit": "MLUPS", "cores": os.cpu_count(), "kind": kind,
+            "sample": f"{sample_steps} coarse steps of {cfg.name} ({cfg.updates_per_step() * sample_steps} updates, "
+                      f"{dt:.1f} s), g++ -O3 -fopenmp, OMP threads = {os.environ.get('OMP_NUM_THREADS', os.cpu_count())}"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    cfg = workload(args)
+    lib, kind = _ref_lib()
+    sim = lib.sim(_ref_case(cfg))
+    budget_s = 150.0
+    for _ in range(min(args.warmup, 1)):
+        sim.run(1)
+    t0 = time.perf_counter()
+    done = 0
+    while done < args.steps:
+        sim.run(1)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    value = cfg.updates_per_step() * done / dt / 1e6
+    sample = (f"{done} of {args.steps} coarse steps of {cfg.name} (time-capped at {budget_s:.0f} s), "
+              f"warm-up {min(args.warmup, 1)} step")
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": done,
+        "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / max(done, 1), 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": cfg.name, "grid": [cfg.nx, cfg.ny, cfg.nz], "refine_block": cfg.refine,
+                   "updates_per_step": cfg.updates_per_step(), "parallelism": "host cores"},
+        "cpu_baseline": {"value": round(value, 2), "unit": "MLUPS", "cores": os.cpu_count(), "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": round(value, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    sim.close()
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_native(args)
+
+
+if __name__ == "__main__":
+    main()

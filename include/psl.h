@@ -1,0 +1,149 @@
+/*
+ * psl.h -- C ABI of the B200-native PeriodicShiftLBM lattice update.
+ *
+ * Drop-in for the reference's per-step update path: each entry point replaces one of the
+ * reference's free functions (cited beside it).  The reference binds these at compile
+ * time (header-only C++/TNL); here they are plain C symbols over an opaque grid handle,
+ * so C++, Python (ctypes) or any FFI can drive them.
+ *
+ * Conventions
+ *   - Every function returns an int status: PSL_OK (0) or a PSL_ERR_* code; the message of
+ *     the last error on the calling thread is psl_last_error().  No exception crosses the
+ *     ABI.
+ *   - A grid owns its device memory (populations, markers, scratch); the caller owns every
+ *     host buffer it passes.
+ *   - All device work of a grid is issued on the grid's CUDA stream (default: the legacy
+ *     default stream; see psl_grid_set_stream) and is stream-ordered; functions that return
+ *     host data synchronise that stream.
+ *   - Grids that exchange data (coarse/fine) must share one stream.
+ *   - There is no CPU fallback: without a usable CUDA device, psl_grid_create fails.
+ */
+#ifndef PSL_H
+#define PSL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSL_OK 0
+#define PSL_ERR_INVALID 1  /* bad argument or inconsistent grid */
+#define PSL_ERR_CUDA 2     /* CUDA runtime error */
+#define PSL_ERR_NOMEM 3    /* device allocation failed */
+#define PSL_ERR_STATE 4    /* device health flag set (non-finite density) or barrier timeout */
+
+typedef struct psl_grid psl_grid;
+
+/* Population storage in HBM.  Arithmetic is FP32 in every form. */
+#define PSL_STORAGE_F32 0       /* f_q as float (216 B moved per cell update) */
+#define PSL_STORAGE_F16_SHIFTED 1  /* f_q - w_q as IEEE half (108 B per cell update) */
+#define PSL_STORAGE_BF16_SHIFTED 2 /* f_q - w_q as bfloat16 (108 B per cell update) */
+
+/* Per-grid metadata; mirrors InfoStruct (include/types.h:73-75). */
+typedef struct psl_info {
+  int grid_id;                 /* refinement level, 0 = coarsest (InfoStruct::gridID) */
+  float res;                   /* cell size in physical units (mm) */
+  int cell_count_x, cell_count_y, cell_count_z;
+  float ox, oy, oz;            /* physical position of cell (0,0,0) */
+  float nu;                    /* lattice kinematic viscosity */
+  float dt_phys;               /* physical time step (s) */
+  int i_subgrid_start, j_subgrid_start, k_subgrid_start; /* finer block on this grid, */
+  int i_subgrid_end, j_subgrid_end, k_subgrid_end;       /* half-open; all 0 = none   */
+} psl_info;
+
+/* The flow-past-sphere case hooks (flowAroundSphere/flowAroundSphereMainSingle.cu:41-92). */
+typedef struct psl_sphere_case {
+  float sphere_x, sphere_y, sphere_z, sphere_r; /* physical units */
+  float u_in;        /* inlet / given velocity (lattice units) */
+  float rho_given;   /* given density at the outlet */
+  int wall_mode;     /* 0: free-slip y/z walls; 1: velocity-given y/z walls (reference driver) */
+  float smagorinsky; /* Smagorinsky constant; 0 disables LES */
+  uint32_t seed;     /* start-state noise seed */
+  float noise_amp;   /* start-state velocity noise amplitude (uniform +-amp) */
+} psl_sphere_case;
+
+/* Marker byte (psl_set_markers): kind in bits 0-2, outer-normal index in bits 3-7,
+ * normal index = (nx+1)*9 + (ny+1)*3 + (nz+1).  For PSL_CELL_SKIP the upper bits are 1 for
+ * a ghost cell (fine-grid boundary layer) and 0 for a refined-interior cell. */
+#define PSL_CELL_SKIP 0
+#define PSL_CELL_FLUID 1
+#define PSL_CELL_SOLID 2
+#define PSL_CELL_GIVEN_U 3
+#define PSL_CELL_GIVEN_RHO 4
+#define PSL_CELL_GIVEN_NONE 5
+#define PSL_CELL_GIVEN_BOTH 6
+#define PSL_CELL_MIRROR 7
+
+/* ---- grid lifetime (replaces GridStruct construction, fArray.setSizes(27, N) and
+ *      shifter = IntArrayType(27, 0): flowAroundSphereMainSingle.cu:171-182) ---- */
+int psl_grid_create(const psl_info* info, int storage, psl_grid** out);
+int psl_grid_destroy(psl_grid* grid);
+int psl_grid_set_stream(psl_grid* grid, void* cuda_stream);
+int psl_grid_get_info(const psl_grid* grid, psl_info* info, long long* cell_count, int* storage);
+
+/* ---- hook equivalents (evaluated once into per-cell markers; see psl_hooks.cuh) ---- */
+/* getMarkers / getGivenRhoUxUyUz / getSmagorinskyConstant of the sphere case. */
+int psl_apply_sphere_case(psl_grid* grid, const psl_sphere_case* sc);
+/* Caller-computed markers, one byte per cell in cell order (i fastest). */
+int psl_set_markers(psl_grid* grid, const uint8_t* host_markers);
+int psl_get_markers(psl_grid* grid, uint8_t* host_markers);
+/* getGivenRhoUxUyUz with one value for every boundary cell. */
+int psl_set_given(psl_grid* grid, float rho, float ux, float uy, float uz);
+/* getGivenRhoUxUyUz per cell: host (rho, ux, uy, uz) x N, or NULL to return to uniform. */
+int psl_set_given_field(psl_grid* grid, const float* host_rho_u);
+/* getSmagorinskyConstant (uniform per grid); 0 disables LES. */
+int psl_set_smagorinsky(psl_grid* grid, float cs);
+
+/* ---- the per-step update ---- */
+/* fillEquilibriumFromFunction (fillEquilibrium.h:1-22) with the sphere case's start hook. */
+int psl_fill_equilibrium_sphere(psl_grid* grid, const psl_sphere_case* sc);
+/* fillEquilibriumFromFunction with a uniform (rho, u). */
+int psl_fill_equilibrium_uniform(psl_grid* grid, float rho, float ux, float uy, float uz);
+/* applyStreaming (applyStreaming.h:11-31): updates the 27 periodic shifts; no kernel. */
+int psl_apply_streaming(psl_grid* grid);
+/* applyLocalCellUpdate (applyLocalCellUpdate.h:1-74): the fused gather / boundary /
+ * cumulant+LES collision / scatter kernel. */
+int psl_apply_local_cell_update(psl_grid* grid);
+/* applyBCPeriodicX / applyBCPeriodicY (boundaryConditions/periodicXY.h:11,57). */
+int psl_apply_bc_periodic_x(psl_grid* grid);
+int psl_apply_bc_periodic_y(psl_grid* grid);
+/* applyCoarseFineGridCommunication (gridRefinementFunctions.h:433-526): one kernel. */
+int psl_apply_coarse_fine_grid_communication(psl_grid* coarse, psl_grid* fine);
+/* updateGrid recursion of the case driver (flowAroundSphereMainSingle.cu:158-167):
+ * streaming + update on grids[level], two steps of level+1, coarse/fine transfer. */
+int psl_update_grid(psl_grid** grids, int levels, int level);
+
+/* ---- reductions (FP64) ---- */
+/* getSphereDrag (flowAroundSphereMainSingle.cu:99-156): momentum exchange summed over
+ * the solid cells of the sphere's bounding box, lattice units of `grid`; force[0] is the
+ * drag (x), force[1..2] the y and z components. */
+int psl_sphere_force(psl_grid* grid, const psl_sphere_case* sc, double* force3);
+
+/* ---- data movement ---- */
+/* Populations in logical order: host[q * N + cell] = f_q of `cell` (FP32 for every storage). */
+int psl_get_populations(psl_grid* grid, float* host);
+int psl_set_populations(psl_grid* grid, const float* host);
+int psl_get_shifts(const psl_grid* grid, int* shifts27);
+int psl_set_shifts(psl_grid* grid, const int* shifts27);
+int psl_synchronize(psl_grid* grid);
+/* Health word of the update kernels (bit 0: non-finite density seen; bit 1: a grid
+ * barrier timed out); read and clear. */
+int psl_check_health(psl_grid* grid, unsigned int* flags);
+
+/* ---- single-cell entry points (unit parity of the device functions) ----
+ * op: 0 collision (args: nu, cs), 1 rescale (a0: coarse_to_fine), 2 MBBC (args: rho,u),
+ * 3 restoreRho, 4 restoreUxUyUz, 5 restoreRhoUxUyUz, 6 mirror, 7 forced collision
+ * (args: nu, cs, gx, gy).  f: count x 27 host floats (in/out), args: count x 4 host floats;
+ * a0: normal index for the boundary ops. */
+int psl_debug_cells(int op, int a0, float* host_f, const float* host_args, int count);
+
+const char* psl_last_error(void);
+const char* psl_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSL_H */

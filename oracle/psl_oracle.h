@@ -1,0 +1,46 @@
+// CPU oracle: the project's own restatement of PeriodicShiftLBM's per-step lattice update.
+//
+// ORACLE / TEST INFRASTRUCTURE ONLY -- the checker, never the thing measured or shipped.
+// Templated on the arithmetic type: T = float reproduces the reference's FP32 update (and
+// is pinned against the reference's own code compiled through oracle/tnl_shim, see
+// oracle/ref_cases.cpp); T = double is the FP64 oracle for the reduced-precision storage
+// forms.  Each function names the reference file:line it restates.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+namespace oracle {
+
+// D3Q27 ordering of the reference (include/applyStreaming.h:1-8,
+// include/cellFunctions.h:3-16): 0 rest, 1-6 faces, 7-18 edges, 19-26 corners,
+// opposite pairs (1,2), (3,4), ..., (25,26).
+constexpr int CX[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, -1, 1, 0, 0, -1, 1, 0, 0, -1, 1, -1, 1, 1, -1, -1, 1};
+constexpr int CY[27] = {0, 0, 0, 0, 0, -1, 1, 0, 0, 0, 0, -1, 1, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1, -1, 1};
+constexpr int CZ[27] = {0, 0, 0, -1, 1, 0, 0, -1, 1, 1, -1, 0, 0, -1, 1, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, -1, 1};
+
+template <typename T>
+struct Weights {
+  static T w(int q) {
+    if (q == 0) return T(8) / T(27);
+    if (q <= 6) return T(2) / T(27);
+    if (q <= 18) return T(1) / T(54);
+    return T(1) / T(216);
+  }
+};
+
+// Case description shared with oracle/ref_cases.cpp (RefCaseConfig): flow past a sphere.
+struct CaseConfig {
+  int nx, ny, nz;
+  int levels;
+  int iSub0, jSub0, kSub0;
+  int iSub1, jSub1, kSub1;
+  float sphereX, sphereY, sphereZ, sphereR;
+  float uIn;
+  float nuCoarse;
+  float smagorinsky;
+  int wallMode;  // 0 free-slip (mirror) y/z walls, 1 velocity walls
+  uint32_t seed;
+  float noiseAmp;
+};
+
+}  // namespace oracle

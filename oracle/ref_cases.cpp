@@ -1,0 +1,409 @@
+// Case driver for the reference solver, compiled for the host.
+//
+// ORACLE / TEST INFRASTRUCTURE ONLY.  This translation unit #includes the reference
+// project's own headers UNMODIFIED (include/types.h, include/cellFunctions.h,
+// include/applyStreaming.h, include/applyCollision.h, include/boundaryConditions/*.h,
+// include/applyLocalCellUpdate.h, include/fillEquilibrium.h,
+// include/gridRefinementFunctions.h, and the free-slip generator output
+// symbolicHelperTools/CppCodeGenerator/results/applyMirror.h that the reference's drivers
+// include but its include/ folder lacks).  It supplies what a reference case file
+// supplies: physical constants, the per-case hook functions (getMarkers,
+// getGivenRhoUxUyUz, getSmagorinskyConstant, getInitialRhoUxUyUz), the updateGrid
+// recursion and a momentum-exchange drag reduction, all written in the reference's own
+// hook style (flowAroundSphere/flowAroundSphereMainSingle.cu:41-167).  TNL comes from the
+// project-written host shim in oracle/tnl_shim (OpenMP parallelFor), so the reference's
+// arithmetic runs on the CPU exactly as written.  The resulting library (oracle/_ref/)
+// pins the project's own oracle restatement and serves as the timed CPU baseline.
+//
+// Hooks read a runtime case description (g_case) so one build serves every sphere
+// configuration: single grid or one 2:1 refinement level, free-slip ("mirror") lateral
+// walls or the reference driver's velocity walls, optional Smagorinsky LES.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+// Physical constants a reference case file defines before including the headers
+// (flowAroundSphere/flowAroundSphereMainSingle.cu:9-13).  Only convertToPhysical* read them.
+float rhoNominalPhys = 1.225f;
+float soundspeedPhys = 1.f;
+constexpr float invSqrt3 = 0.577350269f;
+
+#include "include/types.h"
+
+#include "include/cellFunctions.h"
+#include "include/applyStreaming.h"
+#include "include/applyCollision.h"
+
+#include "include/boundaryConditions/applyBounceback.h"
+#include "include/boundaryConditions/applyMovingBounceback.h"
+#include "applyMirror.h"
+#include "include/boundaryConditions/restoreRho.h"
+#include "include/boundaryConditions/restoreUxUyUz.h"
+#include "include/boundaryConditions/restoreRhoUxUyUz.h"
+#include "include/boundaryConditions/applyMBBC.h"
+
+#include "psl_case_noise.h"
+
+// ---------------------------------------------------------------------------------------
+// Runtime case description (what the reference fixes with constexpr constants per case).
+// ---------------------------------------------------------------------------------------
+extern "C" struct RefCaseConfig {
+  int nx, ny, nz;          // coarse grid cells
+  int levels;              // 1 or 2
+  int iSub0, jSub0, kSub0; // refinement block on the coarse grid (cells, half-open)
+  int iSub1, jSub1, kSub1;
+  float sphereX, sphereY, sphereZ, sphereR;  // in coarse cell units
+  float uIn;
+  float nuCoarse;
+  float smagorinsky;
+  int wallMode;            // 0 = free-slip (mirror) y/z walls, 1 = velocity walls as flowAroundSphere
+  uint32_t seed;
+  float noiseAmp;
+};
+
+static RefCaseConfig g_case;
+
+// Free-slip lateral wall: y or z face cell that is not on the inlet/outlet plane.
+__cuda_callable__ bool isFreeSlipWall(const int& iCell, const int& jCell, const int& kCell, const InfoStruct& Info) {
+  if (g_case.wallMode != 0 || Info.gridID != 0) return false;
+  if (iCell == 0 || iCell == Info.cellCountX - 1) return false;
+  return jCell == 0 || jCell == Info.cellCountY - 1 || kCell == 0 || kCell == Info.cellCountZ - 1;
+}
+
+__cuda_callable__ void getMarkers(const int& iCell, const int& jCell, const int& kCell, MarkerStruct& Marker,
+                                  const InfoStruct& Info) {
+  const float xPhys = iCell * Info.res + Info.ox;
+  const float yPhys = jCell * Info.res + Info.oy;
+  const float zPhys = kCell * Info.res + Info.oz;
+  const float r2 = (xPhys - g_case.sphereX) * (xPhys - g_case.sphereX) +
+                   (yPhys - g_case.sphereY) * (yPhys - g_case.sphereY) +
+                   (zPhys - g_case.sphereZ) * (zPhys - g_case.sphereZ);
+  if (Info.gridID != 0) {
+    if (r2 <= g_case.sphereR * g_case.sphereR) Marker.bounceback = 1;
+    else if (iCell == 0 || iCell == Info.cellCountX - 1) Marker.ghost = 1;
+    else if (jCell == 0 || jCell == Info.cellCountY - 1) Marker.ghost = 1;
+    else if (kCell == 0 || kCell == Info.cellCountZ - 1) Marker.ghost = 1;
+    else Marker.fluid = 1;
+    return;
+  }
+  if (r2 <= g_case.sphereR * g_case.sphereR) { Marker.bounceback = 1; return; }
+  if (g_case.wallMode == 1) {  // order of flowAroundSphereMainSingle.cu:57-64
+    if (jCell == 0 || jCell == Info.cellCountY - 1) Marker.givenUxUyUz = 1;
+    else if (kCell == 0 || kCell == Info.cellCountZ - 1) Marker.givenUxUyUz = 1;
+    else if (iCell == 0) Marker.givenUxUyUz = 1;
+    else if (iCell == Info.cellCountX - 1) Marker.givenRho = 1;
+    else Marker.fluid = 1;
+  } else {  // inlet/outlet planes first, remaining y/z faces are free-slip walls
+    if (iCell == 0) Marker.givenUxUyUz = 1;
+    else if (iCell == Info.cellCountX - 1) Marker.givenRho = 1;
+    else if (isFreeSlipWall(iCell, jCell, kCell, Info)) { /* mirror: no given moments */ }
+    else Marker.fluid = 1;
+  }
+}
+
+__cuda_callable__ void getGivenRhoUxUyUz(const int& iCell, const int& jCell, const int& kCell, float& rho, float& ux,
+                                         float& uy, float& uz, const InfoStruct& Info) {
+  rho = 1.f;
+  ux = g_case.uIn;
+  uy = 0.f;
+  uz = 0.f;
+}
+
+__cuda_callable__ float getSmagorinskyConstant(const int& iCell, const int& jCell, const int& kCell,
+                                               const InfoStruct& Info) {
+  return g_case.smagorinsky;
+}
+
+__cuda_callable__ void getInitialRhoUxUyUz(const int& iCell, const int& jCell, const int& kCell, float& rho, float& ux,
+                                           float& uy, float& uz, const MarkerStruct& Marker, const InfoStruct& Info) {
+  int cell;
+  getCellIndex(cell, iCell, jCell, kCell, Info);
+  const uint32_t level = (uint32_t)Info.gridID;
+  rho = 1.f;
+  ux = psl_noisy_velocity(g_case.uIn, g_case.noiseAmp, g_case.seed, level, (uint32_t)cell, 0);
+  uy = psl_noisy_velocity(0.f, g_case.noiseAmp, g_case.seed, level, (uint32_t)cell, 1);
+  uz = psl_noisy_velocity(0.f, g_case.noiseAmp, g_case.seed, level, (uint32_t)cell, 2);
+}
+
+// DIAD-grid hook overload that the shared DIAD code paths reference; never called here.
+__cuda_callable__ void getGivenRhoUxUyUz(const int& iCell, const int& jCell, const int& kCell, float& rho, float& ux,
+                                         float& uy, float& uz, const InfoStruct& Info, const MarkerStruct& Marker) {
+  getGivenRhoUxUyUz(iCell, jCell, kCell, rho, ux, uy, uz, Info);
+}
+
+#include "include/applyLocalCellUpdate.h"
+#include "include/fillEquilibrium.h"
+#include "include/gridRefinementFunctions.h"
+#include "include/boundaryConditions/periodicXY.h"
+
+// Customized PS update for free-slip walls, in the reference's per-case customisation
+// style (M35Full/m35Main.cu:134-135 swaps in a case's own update): identical to
+// include/applyLocalCellUpdate.h:1-74 except that a free-slip wall cell takes the
+// specular reflection of its unknown populations (applyMirror, as wired in
+// include/scalarTransportFunctions.h:74-77) instead of a moment-based BC.
+void applyLocalCellUpdateFreeSlip(GridStruct& Grid) {
+  auto fArrayView = Grid.fArray.getView();
+  auto shifterView = Grid.shifter.getConstView();
+  InfoStruct Info = Grid.Info;
+  auto cellLambda = [=] __cuda_callable__(const int cell) mutable {
+    int iCell, jCell, kCell;
+    getIJKCellIndex(cell, iCell, jCell, kCell, Info);
+    int shiftedIndex[27];
+    getShiftedIndex(cell, shiftedIndex, shifterView, Info);
+    MarkerStruct Marker;
+    getMarkers(iCell, jCell, kCell, Marker, Info);
+    if (Marker.ghost) return;
+    if ((iCell > Info.iSubgridStart + 1 && iCell < Info.iSubgridEnd - 2) &&
+        (jCell > Info.jSubgridStart + 1 && jCell < Info.jSubgridEnd - 2) &&
+        (kCell > Info.kSubgridStart + 1 && kCell < Info.kSubgridEnd - 2))
+      return;
+    float f[27];
+    float rho, ux, uy, uz;
+    for (int direction = 0; direction < 27; direction++) f[direction] = fArrayView(direction, shiftedIndex[direction]);
+    if (Marker.bounceback) {
+      applyBounceback(f);
+    } else {
+      if (!Marker.fluid) {
+        int outerNormalX, outerNormalY, outerNormalZ;
+        getOuterNormal(iCell, jCell, kCell, outerNormalX, outerNormalY, outerNormalZ, Info);
+        if (Marker.periodicX) outerNormalX = 0;
+        if (Marker.periodicY) outerNormalY = 0;
+        if (Marker.periodicZ) outerNormalZ = 0;
+        getGivenRhoUxUyUz(iCell, jCell, kCell, rho, ux, uy, uz, Info);
+        if (isFreeSlipWall(iCell, jCell, kCell, Info)) {
+          applyMirror(outerNormalX, outerNormalY, outerNormalZ, f);
+        } else {
+          if (Marker.givenRho && !Marker.givenUxUyUz) restoreUxUyUz(outerNormalX, outerNormalY, outerNormalZ, rho, ux, uy, uz, f);
+          else if (!Marker.givenRho && Marker.givenUxUyUz) restoreRho(outerNormalX, outerNormalY, outerNormalZ, rho, ux, uy, uz, f);
+          else if (!Marker.givenRho && !Marker.givenUxUyUz) restoreRhoUxUyUz(outerNormalX, outerNormalY, outerNormalZ, rho, ux, uy, uz, f);
+          applyMBBC(outerNormalX, outerNormalY, outerNormalZ, rho, ux, uy, uz, f);
+        }
+      }
+      const float SmagorinskyConstant = getSmagorinskyConstant(iCell, jCell, kCell, Info);
+      applyCollision(f, Info.nu, SmagorinskyConstant);
+    }
+    for (int direction = 0; direction < 27; direction++) fArrayView(direction, shiftedIndex[direction]) = f[direction];
+  };
+  TNL::Algorithms::parallelFor<TNL::Devices::Cuda>(0, Info.cellCount, cellLambda);
+}
+
+// Momentum-exchange drag over the solid cells in the sphere's bounding box, as the
+// reference driver's getSphereDrag (flowAroundSphereMainSingle.cu:99-156), returned in
+// lattice units of the given grid (before convertToPhysicalForce).
+static double sphereDragLattice(GridStruct& Grid) {
+  auto fArrayView = Grid.fArray.getView();
+  auto shifterView = Grid.shifter.getConstView();
+  InfoStruct Info = Grid.Info;
+  const int iStart = (int)((g_case.sphereX - g_case.sphereR - Info.ox) / Info.res);
+  const int iEnd = (int)((g_case.sphereX + g_case.sphereR - Info.ox) / Info.res) + 2;
+  const int jStart = (int)((g_case.sphereY - g_case.sphereR - Info.oy) / Info.res);
+  const int jEnd = (int)((g_case.sphereY + g_case.sphereR - Info.oy) / Info.res) + 2;
+  const int kStart = (int)((g_case.sphereZ - g_case.sphereR - Info.oz) / Info.res);
+  const int kEnd = (int)((g_case.sphereZ + g_case.sphereR - Info.oz) / Info.res) + 2;
+  const int end = (iEnd - iStart) * (jEnd - jStart) * (kEnd - kStart);
+  auto fetch = [=] __cuda_callable__(const int singleIndex) {
+    const int iSpan = iEnd - iStart;
+    const int jSpan = jEnd - jStart;
+    const int kRelative = singleIndex / (iSpan * jSpan);
+    const int remainder = singleIndex % (iSpan * jSpan);
+    const int iCell = remainder % iSpan + iStart;
+    const int jCell = remainder / iSpan + jStart;
+    const int kCell = kRelative + kStart;
+    int cell;
+    getCellIndex(cell, iCell, jCell, kCell, Info);
+    MarkerStruct Marker;
+    getMarkers(iCell, jCell, kCell, Marker, Info);
+    if (!Marker.bounceback) return 0.f;
+    int shiftedIndex[27];
+    getShiftedIndex(cell, shiftedIndex, shifterView, Info);
+    float f[27];
+    for (int direction = 0; direction < 27; direction++) f[direction] = fArrayView(direction, shiftedIndex[direction]);
+    float rho, ux, uy, uz;
+    getRhoUxUyUz(rho, ux, uy, uz, f);
+    applyBounceback(f);
+    float rhoPrev, uxPrev, uyPrev, uzPrev;
+    getRhoUxUyUz(rhoPrev, uxPrev, uyPrev, uzPrev, f);
+    return rho * (ux - uxPrev);
+  };
+  auto reduction = [] __cuda_callable__(const float& a, const float& b) { return a + b; };
+  return (double)TNL::Algorithms::reduce<TNL::Devices::Cuda>(0, end, fetch, reduction, 0.f);
+}
+
+struct RefSim {
+  std::vector<GridStruct> grids;
+  bool freeSlip = false;
+};
+
+static void updateLevel(RefSim& sim, int level) {
+  std::vector<GridStruct>& grids = sim.grids;
+  applyStreaming(grids[level]);
+  if (sim.freeSlip) applyLocalCellUpdateFreeSlip(grids[level]);
+  else applyLocalCellUpdate(grids[level]);
+  if (level < (int)grids.size() - 1) {  // updateGrid recursion, flowAroundSphereMainSingle.cu:158-167
+    for (int i = 0; i < 2; i++) updateLevel(sim, level + 1);
+    applyCoarseFineGridCommunication(grids[level], grids[level + 1]);
+  }
+}
+
+extern "C" {
+
+void* ref_sim_create(const RefCaseConfig* cfg) {
+  g_case = *cfg;
+  RefSim* sim = new RefSim();
+  sim->freeSlip = (cfg->wallMode == 0);
+  sim->grids.resize(cfg->levels);
+  GridStruct& g0 = sim->grids[0];
+  g0.Info.gridID = 0;
+  g0.Info.res = 1.f;
+  g0.Info.dtPhys = 1.f;
+  g0.Info.nu = cfg->nuCoarse;
+  g0.Info.cellCountX = cfg->nx;
+  g0.Info.cellCountY = cfg->ny;
+  g0.Info.cellCountZ = cfg->nz;
+  g0.Info.cellCount = cfg->nx * cfg->ny * cfg->nz;
+  if (cfg->levels > 1) {
+    g0.Info.iSubgridStart = cfg->iSub0; g0.Info.iSubgridEnd = cfg->iSub1;
+    g0.Info.jSubgridStart = cfg->jSub0; g0.Info.jSubgridEnd = cfg->jSub1;
+    g0.Info.kSubgridStart = cfg->kSub0; g0.Info.kSubgridEnd = cfg->kSub1;
+  }
+  g0.fArray.setSizes(27, g0.Info.cellCount);
+  g0.shifter = IntArrayType(27, 0);
+  fillEquilibriumFromFunction(g0);
+  for (int level = 1; level < cfg->levels; ++level) {  // flowAroundSphereMainSingle.cu:185-220
+    GridStruct& c = sim->grids[level - 1];
+    GridStruct& g = sim->grids[level];
+    g.Info.gridID = c.Info.gridID + 1;
+    g.Info.res = c.Info.res * 0.5f;
+    g.Info.dtPhys = c.Info.dtPhys * 0.5f;
+    g.Info.nu = c.Info.nu * 2.f;  // nu_lattice = dt nu_phys / dx^2
+    g.Info.ox = c.Info.ox + c.Info.iSubgridStart * c.Info.res - g.Info.res * 0.5f;
+    g.Info.oy = c.Info.oy + c.Info.jSubgridStart * c.Info.res - g.Info.res * 0.5f;
+    g.Info.oz = c.Info.oz + c.Info.kSubgridStart * c.Info.res - g.Info.res * 0.5f;
+    g.Info.cellCountX = (c.Info.iSubgridEnd - c.Info.iSubgridStart) * 2;
+    g.Info.cellCountY = (c.Info.jSubgridEnd - c.Info.jSubgridStart) * 2;
+    g.Info.cellCountZ = (c.Info.kSubgridEnd - c.Info.kSubgridStart) * 2;
+    g.Info.cellCount = g.Info.cellCountX * g.Info.cellCountY * g.Info.cellCountZ;
+    g.fArray.setSizes(27, g.Info.cellCount);
+    g.shifter = IntArrayType(27, 0);
+    fillEquilibriumFromFunction(g);
+  }
+  return sim;
+}
+
+void ref_sim_destroy(void* h) { delete static_cast<RefSim*>(h); }
+
+void ref_sim_run(void* h, int steps) {
+  RefSim* sim = static_cast<RefSim*>(h);
+  for (int s = 0; s < steps; ++s) updateLevel(*sim, 0);
+}
+
+long long ref_sim_cell_count(void* h, int level) {
+  return static_cast<RefSim*>(h)->grids[level].Info.cellCount;
+}
+
+void ref_sim_get_info(void* h, int level, float* out_f6, int* out_i10) {
+  const InfoStruct& I = static_cast<RefSim*>(h)->grids[level].Info;
+  out_f6[0] = I.gridID; out_f6[1] = I.res; out_f6[2] = I.ox; out_f6[3] = I.oy; out_f6[4] = I.oz; out_f6[5] = I.nu;
+  out_i10[0] = I.cellCountX; out_i10[1] = I.cellCountY; out_i10[2] = I.cellCountZ; out_i10[3] = I.cellCount;
+  out_i10[4] = I.iSubgridStart; out_i10[5] = I.jSubgridStart; out_i10[6] = I.kSubgridStart;
+  out_i10[7] = I.iSubgridEnd; out_i10[8] = I.jSubgridEnd; out_i10[9] = I.kSubgridEnd;
+}
+
+void ref_sim_get_shifts(void* h, int level, int* out27) {
+  GridStruct& g = static_cast<RefSim*>(h)->grids[level];
+  for (int q = 0; q < 27; ++q) out27[q] = g.shifter[q];
+}
+
+// Populations in logical order: out[q*N + cell] = f_q of `cell` (at its shifted address).
+void ref_sim_get_f(void* h, int level, float* out) {
+  GridStruct& g = static_cast<RefSim*>(h)->grids[level];
+  const long long N = g.Info.cellCount;
+  auto v = g.fArray.getConstView();
+  for (int q = 0; q < 27; ++q) {
+    const long long s = g.shifter[q];
+    for (long long c = 0; c < N; ++c) {
+      long long a = c + s;
+      if (a >= N) a -= N;
+      out[q * N + c] = v(q, (size_t)a);
+    }
+  }
+}
+
+void ref_sim_set_f(void* h, int level, const float* in) {
+  GridStruct& g = static_cast<RefSim*>(h)->grids[level];
+  const long long N = g.Info.cellCount;
+  auto v = g.fArray.getView();
+  for (int q = 0; q < 27; ++q) {
+    const long long s = g.shifter[q];
+    for (long long c = 0; c < N; ++c) {
+      long long a = c + s;
+      if (a >= N) a -= N;
+      v(q, (size_t)a) = in[q * N + c];
+    }
+  }
+}
+
+double ref_sim_drag(void* h) {
+  RefSim* sim = static_cast<RefSim*>(h);
+  return sphereDragLattice(sim->grids.back());
+}
+
+// ---- single-function entry points (unit-level pins) ----
+void ref_collision(float* f, float nu, float cs) {
+  float (&a)[27] = *reinterpret_cast<float (*)[27]>(f);
+  applyCollision(a, nu, cs);
+}
+void ref_feq(float rho, float ux, float uy, float uz, float* out) {
+  getFeq(rho, ux, uy, uz, *reinterpret_cast<float (*)[27]>(out));
+}
+void ref_rho_u(const float* f, float* out4) {
+  getRhoUxUyUz(out4[0], out4[1], out4[2], out4[3], *reinterpret_cast<const float (*)[27]>(f));
+}
+void ref_omega_les(const float* f, float nu, float cs, float* omega) {
+  float rho, ux, uy, uz, feq[27], fneq[27];
+  const float (&a)[27] = *reinterpret_cast<const float (*)[27]>(f);
+  getRhoUxUyUz(rho, ux, uy, uz, a);
+  getFeq(rho, ux, uy, uz, feq);
+  getFneq(a, feq, fneq);
+  getOmegaLES(fneq, rho, nu, cs, *omega);
+}
+void ref_mbbc(int nx, int ny, int nz, float rho, float ux, float uy, float uz, float* f) {
+  applyMBBC(nx, ny, nz, rho, ux, uy, uz, *reinterpret_cast<float (*)[27]>(f));
+}
+void ref_restore_rho(int nx, int ny, int nz, float ux, float uy, float uz, const float* f, float* rho) {
+  restoreRho(nx, ny, nz, *rho, ux, uy, uz, *reinterpret_cast<const float (*)[27]>(f));
+}
+void ref_restore_u(int nx, int ny, int nz, float rho, const float* f, float* u3) {
+  restoreUxUyUz(nx, ny, nz, rho, u3[0], u3[1], u3[2], *reinterpret_cast<const float (*)[27]>(f));
+}
+void ref_restore_rho_u(int nx, int ny, int nz, const float* f, float* out4) {
+  restoreRhoUxUyUz(nx, ny, nz, out4[0], out4[1], out4[2], out4[3], *reinterpret_cast<const float (*)[27]>(f));
+}
+void ref_mirror(int nx, int ny, int nz, float* f) { applyMirror(nx, ny, nz, *reinterpret_cast<float (*)[27]>(f)); }
+void ref_bounceback(float* f) { applyBounceback(*reinterpret_cast<float (*)[27]>(f)); }
+void ref_moving_bounceback(float* f, float ux, float uy, float uz) {
+  applyMovingBounceback(*reinterpret_cast<float (*)[27]>(f), ux, uy, uz);
+}
+void ref_rescale(float* f, int coarseToFine) {
+  const bool c2f = coarseToFine != 0;
+  rescaleF(*reinterpret_cast<float (*)[27]>(f), c2f);
+}
+// applyStreaming on a bare grid of the given size, starting from the given shifts.
+void ref_streaming(int nx, int ny, int nz, int* shifts27) {
+  GridStruct g;
+  g.Info.cellCountX = nx; g.Info.cellCountY = ny; g.Info.cellCountZ = nz;
+  g.Info.cellCount = nx * ny * nz;
+  g.shifter = IntArrayType(27, 0);
+  for (int q = 0; q < 27; ++q) g.shifter[q] = shifts27[q];
+  applyStreaming(g);
+  for (int q = 0; q < 27; ++q) shifts27[q] = g.shifter[q];
+}
+// applyBCPeriodicX / Y on a simulation grid (in place).
+void ref_sim_periodic_x(void* h, int level) { applyBCPeriodicX(static_cast<RefSim*>(h)->grids[level]); }
+void ref_sim_periodic_y(void* h, int level) { applyBCPeriodicY(static_cast<RefSim*>(h)->grids[level]); }
+void ref_sim_streaming(void* h, int level) { applyStreaming(static_cast<RefSim*>(h)->grids[level]); }
+
+}  // extern "C"

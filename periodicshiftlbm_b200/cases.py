@@ -1,0 +1,96 @@
+"""Flow-past-sphere configurations: grid metadata, hooks and start state.
+
+* ``config1``: 128x64x64 single grid, sphere D=16 at (32,32,32), u_in=0.05, nu=0.008
+  (Re=100), no LES, free-slip y/z walls, velocity inlet at x=0, pressure outlet at x=127.
+* ``config2``: 512x256x256 coarse grid with one 2:1 refinement level over the coarse block
+  [80,208) x [80,176) x [80,176) (128x96x96 coarse cells -> 256x192x192 fine cells),
+  sphere D=48 at (128,128,128), Re=1e5 (nu_coarse = 0.05*48/1e5 = 2.4e-5, nu_fine = 2 nu),
+  Smagorinsky C_s=0.1, same boundary conditions.
+
+Both start from feq(rho=1, u_in + U(+-1e-4)) with a seeded counter-based noise.  Lengths
+are in coarse-cell units (res=1 on the coarse grid).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, replace
+
+from .grid import GridStruct, InfoStruct, SphereCase, fillEquilibriumFromFunction, setSphereCase
+
+
+@dataclass(frozen=True)
+class SphereConfig:
+    name: str
+    nx: int
+    ny: int
+    nz: int
+    sphere: tuple
+    radius: float
+    u_in: float
+    nu: float
+    smagorinsky: float = 0.0
+    wall_mode: int = 0
+    seed: int = 1234
+    noise: float = 1e-4
+    refine: tuple | None = None  # ((i0, j0, k0), (i1, j1, k1)) coarse block, half-open
+
+    def case(self) -> SphereCase:
+        return SphereCase(sphere=tuple(float(v) for v in self.sphere), radius=float(self.radius), u_in=self.u_in,
+                          rho_given=1.0, wall_mode=self.wall_mode, smagorinsky=self.smagorinsky, seed=self.seed,
+                          noise=self.noise)
+
+    def infos(self) -> list:
+        c = InfoStruct(gridID=0, res=1.0, cellCountX=self.nx, cellCountY=self.ny, cellCountZ=self.nz, nu=self.nu)
+        out = [c]
+        if self.refine:
+            (c.iSubgridStart, c.jSubgridStart, c.kSubgridStart), (c.iSubgridEnd, c.jSubgridEnd, c.kSubgridEnd) = self.refine
+            out.append(c.finer())
+        return out
+
+    def updates_per_step(self) -> int:
+        """Cells actually updated per coarse step: every non-skipped coarse cell plus two
+        fine steps of the fine interior (the fine grid's one-cell ghost layer and the coarse
+        refined interior are not updated, include/applyLocalCellUpdate.h:25-30)."""
+        n = self.nx * self.ny * self.nz
+        if not self.refine:
+            return n
+        (i0, j0, k0), (i1, j1, k1) = self.refine
+        interior = max(0, i1 - i0 - 4) * max(0, j1 - j0 - 4) * max(0, k1 - k0 - 4)
+        fx, fy, fz = 2 * (i1 - i0), 2 * (j1 - j0), 2 * (k1 - k0)
+        return n - interior + 2 * (fx - 2) * (fy - 2) * (fz - 2)
+
+    def reference_updates_per_step(self) -> int:
+        """The reference driver's own count (flowAroundSphereMainSingle.cu:225-234), which
+        subtracts (n-2)^3 per refined block instead of the (n-4)^3 cells it skips and
+        counts the fine ghost layer."""
+        n = self.nx * self.ny * self.nz
+        if not self.refine:
+            return n
+        (i0, j0, k0), (i1, j1, k1) = self.refine
+        fx, fy, fz = 2 * (i1 - i0), 2 * (j1 - j0), 2 * (k1 - k0)
+        return n - (i1 - i0 - 2) * (j1 - j0 - 2) * (k1 - k0 - 2) + 2 * fx * fy * fz
+
+
+def config1(**kw) -> SphereConfig:
+    c = SphereConfig(name="sphere_128x64x64_re100", nx=128, ny=64, nz=64, sphere=(32.0, 32.0, 32.0), radius=8.0,
+                     u_in=0.05, nu=0.05 * 16 / 100)
+    return replace(c, **kw)
+
+
+def config2(**kw) -> SphereConfig:
+    c = SphereConfig(name="sphere_512x256x256_re1e5_refined", nx=512, ny=256, nz=256, sphere=(128.0, 128.0, 128.0),
+                     radius=24.0, u_in=0.05, nu=0.05 * 48 / 1e5, smagorinsky=0.1,
+                     refine=((80, 80, 80), (208, 176, 176)))
+    return replace(c, **kw)
+
+
+def make_sphere_grids(cfg: SphereConfig, storage: str = "f32") -> tuple:
+    """Allocate the grids of `cfg`, evaluate the case hooks into markers and fill the
+    start state.  Returns (grids, case)."""
+    case = cfg.case()
+    grids = []
+    for info in cfg.infos():
+        g = GridStruct(info, storage=storage if info.gridID == 0 or storage == "f32" else storage)
+        setSphereCase(g, case)
+        fillEquilibriumFromFunction(g, case)
+        grids.append(g)
+    return grids, case

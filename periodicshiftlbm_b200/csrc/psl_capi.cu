@@ -1,0 +1,575 @@
+// C ABI of the lattice update (include/psl.h): grid handles, set-up, per-step launches,
+// reductions and data movement.  Host-side logic only; the kernels are in psl_kernels.cuh.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "psl.h"
+#include "psl_kernels.cuh"
+
+using namespace psl;
+
+// ------------------------------------------------------------------------------------------
+// errors
+// ------------------------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define PSL_CUDA(expr)                                                                                 \
+  do {                                                                                                 \
+    cudaError_t e_ = (expr);                                                                           \
+    if (e_ != cudaSuccess) return fail(PSL_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define PSL_CHECK(cond, code, msg) \
+  do {                             \
+    if (!(cond)) return fail(code, msg); \
+  } while (0)
+
+// Make the grid's device current for the duration of a call, restoring the caller's.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) ok = (cudaSetDevice(dev) == cudaSuccess);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// ------------------------------------------------------------------------------------------
+// grid
+// ------------------------------------------------------------------------------------------
+struct psl_grid {
+  psl_info info;
+  uint32_t n = 0;
+  int storage = 0;
+  size_t stride = 0;  // elements per population row, multiple of 64 (128-byte rows)
+  void* f = nullptr;
+  uint8_t* marker = nullptr;
+  float4* given = nullptr;
+  float4 given_uniform = make_float4(1.f, 0.f, 0.f, 0.f);
+  float cs = 0.f;
+  uint32_t shift[27] = {};
+  cudaStream_t stream = 0;
+  unsigned int* health = nullptr;   // [0] health bits, [1] barrier counter
+  double* scratch = nullptr;        // force partials (kForceBlocks x 3) + result (3)
+  int device = 0;
+};
+
+static constexpr int kForceBlocks = 512;
+
+template <typename S>
+static GridView<S> view(const psl_grid* g) {
+  GridView<S> v;
+  typename S::type* base = static_cast<typename S::type*>(g->f);
+  for (int q = 0; q < 27; ++q) {
+    v.fq[q] = base + (size_t)q * g->stride;
+    v.shift[q] = g->shift[q];
+  }
+  v.n = g->n;
+  return v;
+}
+
+static InfoStruct hook_info(const psl_grid* g) {
+  InfoStruct I;
+  I.gridID = (float)g->info.grid_id;
+  I.res = g->info.res;
+  I.cellCountX = g->info.cell_count_x;
+  I.cellCountY = g->info.cell_count_y;
+  I.cellCountZ = g->info.cell_count_z;
+  I.cellCount = (int)g->n;
+  I.ox = g->info.ox;
+  I.oy = g->info.oy;
+  I.oz = g->info.oz;
+  I.nu = g->info.nu;
+  I.dtPhys = g->info.dt_phys;
+  I.iSubgridStart = g->info.i_subgrid_start;
+  I.jSubgridStart = g->info.j_subgrid_start;
+  I.kSubgridStart = g->info.k_subgrid_start;
+  I.iSubgridEnd = g->info.i_subgrid_end;
+  I.jSubgridEnd = g->info.j_subgrid_end;
+  I.kSubgridEnd = g->info.k_subgrid_end;
+  return I;
+}
+
+static SphereCase sphere_hooks(const psl_sphere_case* sc) {
+  SphereCase c;
+  c.sx = sc->sphere_x;
+  c.sy = sc->sphere_y;
+  c.sz = sc->sphere_z;
+  c.r = sc->sphere_r;
+  c.uIn = sc->u_in;
+  c.rhoGiven = sc->rho_given;
+  c.wallMode = sc->wall_mode;
+  c.smagorinsky = sc->smagorinsky;
+  c.seed = sc->seed;
+  c.noiseAmp = sc->noise_amp;
+  return c;
+}
+
+static unsigned int blocks_for(size_t n, int threads) { return (unsigned int)((n + threads - 1) / threads); }
+
+// Every psl_* definition below takes C linkage from its declaration in psl.h.
+
+const char* psl_last_error(void) { return g_last_error.c_str(); }
+const char* psl_version(void) { return "periodicshiftlbm_b200 0.1 (sm_100a)"; }
+
+int psl_grid_create(const psl_info* info, int storage, psl_grid** out) {
+  PSL_CHECK(info && out, PSL_ERR_INVALID, "psl_grid_create: null argument");
+  *out = nullptr;
+  const long long nx = info->cell_count_x, ny = info->cell_count_y, nz = info->cell_count_z;
+  PSL_CHECK(nx > 0 && ny > 0 && nz > 0, PSL_ERR_INVALID, "psl_grid_create: cell counts must be positive");
+  const long long n = nx * ny * nz;
+  // the reference's shift normalisation (applyStreaming.h:24-27) wraps at most twice,
+  // which covers every grid except Ny = Nz = 1
+  PSL_CHECK(!(ny == 1 && nz == 1), PSL_ERR_INVALID, "psl_grid_create: Ny = Nz = 1 grids are not supported");
+  PSL_CHECK(n < (1LL << 31), PSL_ERR_INVALID, "psl_grid_create: more than 2^31-1 cells");
+  PSL_CHECK(storage >= 0 && storage <= 2, PSL_ERR_INVALID, "psl_grid_create: unknown storage");
+  const bool has_block = info->i_subgrid_end > info->i_subgrid_start;
+  if (has_block) {
+    PSL_CHECK(info->i_subgrid_start >= 0 && info->i_subgrid_end <= nx && info->j_subgrid_start >= 0 &&
+                  info->j_subgrid_end <= ny && info->k_subgrid_start >= 0 && info->k_subgrid_end <= nz,
+              PSL_ERR_INVALID, "psl_grid_create: refinement block outside the grid");
+  }
+  int ndev = 0;
+  PSL_CUDA(cudaGetDeviceCount(&ndev));
+  PSL_CHECK(ndev > 0, PSL_ERR_CUDA, "psl_grid_create: no CUDA device");
+  psl_grid* g = new psl_grid();
+  g->info = *info;
+  g->n = (uint32_t)n;
+  g->storage = storage;
+  g->stride = ((size_t)n + 63) / 64 * 64;
+  cudaGetDevice(&g->device);
+  const size_t bytes = 27 * g->stride * storage_bytes(storage);
+  cudaError_t e = cudaMalloc(&g->f, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&g->marker, g->stride);
+  if (e == cudaSuccess) e = cudaMalloc(&g->health, 4 * sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMalloc(&g->scratch, (kForceBlocks * 3 + 3) * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemset(g->marker, make_marker(kFluid, 0), g->stride);
+  if (e == cudaSuccess) e = cudaMemset(g->health, 0, 4 * sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemset(g->f, 0, bytes);
+  if (e != cudaSuccess) {
+    const std::string msg = std::string("psl_grid_create: ") + cudaGetErrorString(e);
+    psl_grid_destroy(g);
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? PSL_ERR_NOMEM : PSL_ERR_CUDA, msg);
+  }
+  *out = g;
+  return PSL_OK;
+}
+
+int psl_grid_destroy(psl_grid* g) {
+  if (!g) return PSL_OK;
+  DeviceGuard dg(g->device);
+  if (g->f) cudaFree(g->f);
+  if (g->marker) cudaFree(g->marker);
+  if (g->given) cudaFree(g->given);
+  if (g->health) cudaFree(g->health);
+  if (g->scratch) cudaFree(g->scratch);
+  delete g;
+  return PSL_OK;
+}
+
+int psl_grid_set_stream(psl_grid* g, void* stream) {
+  PSL_CHECK(g, PSL_ERR_INVALID, "psl_grid_set_stream: null grid");
+  g->stream = static_cast<cudaStream_t>(stream);
+  return PSL_OK;
+}
+
+int psl_grid_get_info(const psl_grid* g, psl_info* info, long long* cell_count, int* storage) {
+  PSL_CHECK(g, PSL_ERR_INVALID, "psl_grid_get_info: null grid");
+  if (info) *info = g->info;
+  if (cell_count) *cell_count = g->n;
+  if (storage) *storage = g->storage;
+  return PSL_OK;
+}
+
+// ---- hooks ----
+int psl_apply_sphere_case(psl_grid* g, const psl_sphere_case* sc) {
+  PSL_CHECK(g && sc, PSL_ERR_INVALID, "psl_apply_sphere_case: null argument");
+  DeviceGuard dg(g->device);
+  fill_markers_kernel<SphereCase><<<blocks_for(g->n, 256), 256, 0, g->stream>>>(sphere_hooks(sc), hook_info(g), g->n,
+                                                                                 g->marker, nullptr);
+  PSL_CUDA(cudaGetLastError());
+  g->given_uniform = make_float4(sc->rho_given, sc->u_in, 0.f, 0.f);
+  g->cs = sc->smagorinsky;
+  return PSL_OK;
+}
+
+int psl_set_markers(psl_grid* g, const uint8_t* host) {
+  PSL_CHECK(g && host, PSL_ERR_INVALID, "psl_set_markers: null argument");
+  DeviceGuard dg(g->device);
+  PSL_CUDA(cudaMemcpyAsync(g->marker, host, g->n, cudaMemcpyHostToDevice, g->stream));
+  PSL_CUDA(cudaStreamSynchronize(g->stream));
+  return PSL_OK;
+}
+
+int psl_get_markers(psl_grid* g, uint8_t* host) {
+  PSL_CHECK(g && host, PSL_ERR_INVALID, "psl_get_markers: null argument");
+  DeviceGuard dg(g->device);
+  PSL_CUDA(cudaMemcpyAsync(host, g->marker, g->n, cudaMemcpyDeviceToHost, g->stream));
+  PSL_CUDA(cudaStreamSynchronize(g->stream));
+  return PSL_OK;
+}
+
+int psl_set_given(psl_grid* g, float rho, float ux, float uy, float uz) {
+  PSL_CHECK(g, PSL_ERR_INVALID, "psl_set_given: null grid");
+  g->given_uniform = make_float4(rho, ux, uy, uz);
+  return PSL_OK;
+}
+
+int psl_set_given_field(psl_grid* g, const float* host) {
+  PSL_CHECK(g, PSL_ERR_INVALID, "psl_set_given_field: null grid");
+  DeviceGuard dg(g->device);
+  if (!host) {
+    if (g->given) {
+      PSL_CUDA(cudaStreamSynchronize(g->stream));
+      cudaFree(g->given);
+      g->given = nullptr;
+    }
+    return PSL_OK;
+  }
+  if (!g->given) {
+    cudaError_t e = cudaMalloc(&g->given, (size_t)g->n * sizeof(float4));
+    if (e != cudaSuccess) {
+      g->given = nullptr;
+      cudaGetLastError();
+      return fail(PSL_ERR_NOMEM, std::string("psl_set_given_field: ") + cudaGetErrorString(e));
+    }
+  }
+  PSL_CUDA(cudaMemcpyAsync(g->given, host, (size_t)g->n * sizeof(float4), cudaMemcpyHostToDevice, g->stream));
+  PSL_CUDA(cudaStreamSynchronize(g->stream));
+  return PSL_OK;
+}
+
+int psl_set_smagorinsky(psl_grid* g, float cs) {
+  PSL_CHECK(g, PSL_ERR_INVALID, "psl_set_smagorinsky: null grid");
+  g->cs = cs;
+  return PSL_OK;
+}
+
+// ---- per-step update ----
+template <typename Case>
+static int fill_eq(psl_grid* g, const Case& c) {
+  DeviceGuard dg(g->device);
+  const unsigned int nb = blocks_for(g->n, 256);
+  switch (g->storage) {
+    case kStoreF32: fill_equilibrium_kernel<StoreF32, Case><<<nb, 256, 0, g->stream>>>(view<StoreF32>(g), c, hook_info(g)); break;
+    case kStoreF16: fill_equilibrium_kernel<StoreF16, Case><<<nb, 256, 0, g->stream>>>(view<StoreF16>(g), c, hook_info(g)); break;
+    default: fill_equilibrium_kernel<StoreBF16, Case><<<nb, 256, 0, g->stream>>>(view<StoreBF16>(g), c, hook_info(g)); break;
+  }
+  PSL_CUDA(cudaGetLastError());
+  return PSL_OK;
+}
+
+int psl_fill_equilibrium_sphere(psl_grid* g, const psl_sphere_case* sc) {
+  PSL_CHECK(g && sc, PSL_ERR_INVALID, "psl_fill_equilibrium_sphere: null argument");
+  return fill_eq(g, sphere_hooks(sc));
+}
+
+int psl_fill_equilibrium_uniform(psl_grid* g, float rho, float ux, float uy, float uz) {
+  PSL_CHECK(g, PSL_ERR_INVALID, "psl_fill_equilibrium_uniform: null grid");
+  UniformCase c{rho, ux, uy, uz};
+  return fill_eq(g, c);
+}
+
+int psl_apply_streaming(psl_grid* g) {
+  PSL_CHECK(g, PSL_ERR_INVALID, "psl_apply_streaming: null grid");
+  const long long nx = g->info.cell_count_x, ny = g->info.cell_count_y, n = g->n;
+  for (int q = 0; q < 27; ++q) {
+    long long s = (long long)g->shift[q];
+    s -= cx(q);
+    s -= nx * cy(q);
+    s -= ny * nx * cz(q);
+    if (s < 0) s += n;
+    if (s < 0) s += n;
+    if (s >= n) s -= n;
+    if (s >= n) s -= n;
+    g->shift[q] = (uint32_t)s;
+  }
+  return PSL_OK;
+}
+
+static Relaxation relaxation(const psl_grid* g) {
+  Relaxation rx;
+  rx.tau = 3.f * g->info.nu + 0.5f;
+  rx.tau2 = rx.tau * rx.tau;
+  rx.omega0 = 1.f / rx.tau;
+  rx.cs18 = 18.f * g->cs;
+  return rx;
+}
+
+template <typename S>
+static void launch_step(psl_grid* g) {
+  StepParams<S> p;
+  p.g = view<S>(g);
+  p.marker = g->marker;
+  p.given = g->given;
+  p.given_uniform = g->given_uniform;
+  p.rx = relaxation(g);
+  p.health = g->health;
+  step_kernel<S><<<blocks_for(g->n, kStepThreads), kStepThreads, 0, g->stream>>>(p);
+}
+
+int psl_apply_local_cell_update(psl_grid* g) {
+  PSL_CHECK(g, PSL_ERR_INVALID, "psl_apply_local_cell_update: null grid");
+  DeviceGuard dg(g->device);
+  switch (g->storage) {
+    case kStoreF32: launch_step<StoreF32>(g); break;
+    case kStoreF16: launch_step<StoreF16>(g); break;
+    default: launch_step<StoreBF16>(g); break;
+  }
+  PSL_CUDA(cudaGetLastError());
+  return PSL_OK;
+}
+
+template <typename S>
+static void launch_periodic(psl_grid* g, int axis) {
+  const int nx = g->info.cell_count_x, ny = g->info.cell_count_y, nz = g->info.cell_count_z;
+  const int items = (axis == 0 ? ny : nx) * nz;
+  if (axis == 0)
+    periodic_kernel<S, 0><<<blocks_for(items, 256), 256, 0, g->stream>>>(view<S>(g), nx, ny, nz);
+  else
+    periodic_kernel<S, 1><<<blocks_for(items, 256), 256, 0, g->stream>>>(view<S>(g), nx, ny, nz);
+}
+
+static int periodic(psl_grid* g, int axis) {
+  PSL_CHECK(g, PSL_ERR_INVALID, "psl_apply_bc_periodic: null grid");
+  DeviceGuard dg(g->device);
+  switch (g->storage) {
+    case kStoreF32: launch_periodic<StoreF32>(g, axis); break;
+    case kStoreF16: launch_periodic<StoreF16>(g, axis); break;
+    default: launch_periodic<StoreBF16>(g, axis); break;
+  }
+  PSL_CUDA(cudaGetLastError());
+  return PSL_OK;
+}
+int psl_apply_bc_periodic_x(psl_grid* g) { return periodic(g, 0); }
+int psl_apply_bc_periodic_y(psl_grid* g) { return periodic(g, 1); }
+
+int psl_apply_coarse_fine_grid_communication(psl_grid* c, psl_grid* f) {
+  PSL_CHECK(c && f, PSL_ERR_INVALID, "psl_apply_coarse_fine_grid_communication: null grid");
+  PSL_CHECK(c->storage == kStoreF32 && f->storage == kStoreF32, PSL_ERR_INVALID,
+            "psl_apply_coarse_fine_grid_communication: refinement needs FP32 storage");
+  const psl_info& C = c->info;
+  const psl_info& F = f->info;
+  const int a = C.i_subgrid_end - C.i_subgrid_start, b = C.j_subgrid_end - C.j_subgrid_start,
+            cc = C.k_subgrid_end - C.k_subgrid_start;
+  PSL_CHECK(a >= 4 && b >= 4 && cc >= 4, PSL_ERR_INVALID, "coarse/fine: refinement block needs >= 4 cells per axis");
+  PSL_CHECK(F.cell_count_x == 2 * a && F.cell_count_y == 2 * b && F.cell_count_z == 2 * cc, PSL_ERR_INVALID,
+            "coarse/fine: fine grid is not twice the refinement block");
+  PSL_CHECK(c->device == f->device, PSL_ERR_INVALID, "coarse/fine: grids on different devices");
+  DeviceGuard dg(c->device);
+  CoarseFineParams p;
+  p.c = view<StoreF32>(c);
+  p.f = view<StoreF32>(f);
+  p.cnx = C.cell_count_x;
+  p.cny = C.cell_count_y;
+  p.cnz = C.cell_count_z;
+  p.iS = C.i_subgrid_start; p.jS = C.j_subgrid_start; p.kS = C.k_subgrid_start;
+  p.iE = C.i_subgrid_end; p.jE = C.j_subgrid_end; p.kE = C.k_subgrid_end;
+  p.fnx = F.cell_count_x;
+  p.fny = F.cell_count_y;
+  p.fnz = F.cell_count_z;
+  p.fine_marker = f->marker;
+  p.face_active = 0;
+  if (p.iS > 0) p.face_active |= 1;
+  if (p.iE < p.cnx - 1) p.face_active |= 2;
+  if (p.jS > 0) p.face_active |= 4;
+  if (p.jE < p.cny - 1) p.face_active |= 8;
+  if (p.kS > 0) p.face_active |= 16;
+  if (p.kE < p.cnz - 1) p.face_active |= 32;
+  const long long ra = a - 2, rb = b - 2, rc = cc - 2;
+  p.n_ring = (uint32_t)(ra * rb * rc - (ra - 2) * (rb - 2) * (rc - 2));
+  p.n_shell = (uint32_t)((long long)p.fnx * p.fny * p.fnz - (long long)(p.fnx - 4) * (p.fny - 4) * (p.fnz - 4));
+  p.barrier = c->health + 1;
+  p.error = c->health;
+  int sms = 0, per_sm = 0;
+  PSL_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+  PSL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_fine_kernel, 256, 0));
+  PSL_CHECK(per_sm > 0, PSL_ERR_CUDA, "coarse/fine: kernel cannot be resident");
+  const unsigned int want = blocks_for(std::max(p.n_ring, p.n_shell), 256);
+  p.nblocks = std::min<unsigned int>((unsigned int)(sms * per_sm), std::max(1u, want));
+  PSL_CUDA(cudaMemsetAsync(p.barrier, 0, sizeof(unsigned int), c->stream));
+  void* args[] = {&p};
+  PSL_CUDA(cudaLaunchCooperativeKernel((const void*)coarse_fine_kernel, dim3(p.nblocks), dim3(256), args, 0, c->stream));
+  return PSL_OK;
+}
+
+int psl_update_grid(psl_grid** grids, int levels, int level) {
+  PSL_CHECK(grids && levels > 0 && level >= 0 && level < levels, PSL_ERR_INVALID, "psl_update_grid: bad levels");
+  int rc = psl_apply_streaming(grids[level]);
+  if (rc) return rc;
+  rc = psl_apply_local_cell_update(grids[level]);
+  if (rc) return rc;
+  if (level < levels - 1) {
+    for (int i = 0; i < 2; ++i) {
+      rc = psl_update_grid(grids, levels, level + 1);
+      if (rc) return rc;
+    }
+    rc = psl_apply_coarse_fine_grid_communication(grids[level], grids[level + 1]);
+    if (rc) return rc;
+  }
+  return PSL_OK;
+}
+
+// ---- reductions ----
+template <typename S>
+static void launch_force(psl_grid* g, int i0, int j0, int k0, int si, int sj, int sk, int nb) {
+  force_partial_kernel<S><<<nb, 256, 0, g->stream>>>(view<S>(g), g->marker, g->info.cell_count_x,
+                                                     g->info.cell_count_y, i0, j0, k0, si, sj, sk, g->scratch);
+}
+
+int psl_sphere_force(psl_grid* g, const psl_sphere_case* sc, double* force3) {
+  PSL_CHECK(g && sc && force3, PSL_ERR_INVALID, "psl_sphere_force: null argument");
+  DeviceGuard dg(g->device);
+  const psl_info& I = g->info;
+  // bounding box as getSphereDrag computes it (flowAroundSphereMainSingle.cu:105-110)
+  int i0 = (int)((sc->sphere_x - sc->sphere_r - I.ox) / I.res);
+  int i1 = (int)((sc->sphere_x + sc->sphere_r - I.ox) / I.res) + 2;
+  int j0 = (int)((sc->sphere_y - sc->sphere_r - I.oy) / I.res);
+  int j1 = (int)((sc->sphere_y + sc->sphere_r - I.oy) / I.res) + 2;
+  int k0 = (int)((sc->sphere_z - sc->sphere_r - I.oz) / I.res);
+  int k1 = (int)((sc->sphere_z + sc->sphere_r - I.oz) / I.res) + 2;
+  i0 = std::max(i0, 0); j0 = std::max(j0, 0); k0 = std::max(k0, 0);
+  i1 = std::min(i1, I.cell_count_x); j1 = std::min(j1, I.cell_count_y); k1 = std::min(k1, I.cell_count_z);
+  force3[0] = force3[1] = force3[2] = 0.0;
+  if (i1 <= i0 || j1 <= j0 || k1 <= k0) return PSL_OK;
+  const int si = i1 - i0, sj = j1 - j0, sk = k1 - k0;
+  const int nb = (int)std::min<long long>(kForceBlocks, ((long long)si * sj * sk + 255) / 256);
+  switch (g->storage) {
+    case kStoreF32: launch_force<StoreF32>(g, i0, j0, k0, si, sj, sk, nb); break;
+    case kStoreF16: launch_force<StoreF16>(g, i0, j0, k0, si, sj, sk, nb); break;
+    default: launch_force<StoreBF16>(g, i0, j0, k0, si, sj, sk, nb); break;
+  }
+  force_final_kernel<<<1, 32, 0, g->stream>>>(g->scratch, nb, g->scratch + kForceBlocks * 3);
+  PSL_CUDA(cudaGetLastError());
+  PSL_CUDA(cudaMemcpyAsync(force3, g->scratch + kForceBlocks * 3, 3 * sizeof(double), cudaMemcpyDeviceToHost, g->stream));
+  PSL_CUDA(cudaStreamSynchronize(g->stream));
+  return PSL_OK;
+}
+
+// ---- data movement ----
+template <typename S>
+static int gather(psl_grid* g, float* host) {
+  float* tmp = nullptr;
+  PSL_CUDA(cudaMalloc(&tmp, (size_t)g->n * sizeof(float)));
+  cudaError_t e = cudaSuccess;
+  const GridView<S> v = view<S>(g);
+  for (int q = 0; q < 27 && e == cudaSuccess; ++q) {
+    gather_logical_kernel<S><<<blocks_for(g->n, 256), 256, 0, g->stream>>>(v, q, tmp);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(host + (size_t)q * g->n, tmp, (size_t)g->n * sizeof(float), cudaMemcpyDeviceToHost, g->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  }
+  cudaFree(tmp);
+  if (e != cudaSuccess) return fail(PSL_ERR_CUDA, std::string("psl_get_populations: ") + cudaGetErrorString(e));
+  return PSL_OK;
+}
+
+template <typename S>
+static int scatter(psl_grid* g, const float* host) {
+  float* tmp = nullptr;
+  PSL_CUDA(cudaMalloc(&tmp, (size_t)g->n * sizeof(float)));
+  cudaError_t e = cudaSuccess;
+  const GridView<S> v = view<S>(g);
+  for (int q = 0; q < 27 && e == cudaSuccess; ++q) {
+    e = cudaMemcpyAsync(tmp, host + (size_t)q * g->n, (size_t)g->n * sizeof(float), cudaMemcpyHostToDevice, g->stream);
+    if (e == cudaSuccess) {
+      scatter_logical_kernel<S><<<blocks_for(g->n, 256), 256, 0, g->stream>>>(v, q, tmp);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  }
+  cudaFree(tmp);
+  if (e != cudaSuccess) return fail(PSL_ERR_CUDA, std::string("psl_set_populations: ") + cudaGetErrorString(e));
+  return PSL_OK;
+}
+
+int psl_get_populations(psl_grid* g, float* host) {
+  PSL_CHECK(g && host, PSL_ERR_INVALID, "psl_get_populations: null argument");
+  DeviceGuard dg(g->device);
+  PSL_CUDA(cudaStreamSynchronize(g->stream));
+  switch (g->storage) {
+    case kStoreF32: return gather<StoreF32>(g, host);
+    case kStoreF16: return gather<StoreF16>(g, host);
+    default: return gather<StoreBF16>(g, host);
+  }
+}
+
+int psl_set_populations(psl_grid* g, const float* host) {
+  PSL_CHECK(g && host, PSL_ERR_INVALID, "psl_set_populations: null argument");
+  DeviceGuard dg(g->device);
+  PSL_CUDA(cudaStreamSynchronize(g->stream));
+  switch (g->storage) {
+    case kStoreF32: return scatter<StoreF32>(g, host);
+    case kStoreF16: return scatter<StoreF16>(g, host);
+    default: return scatter<StoreBF16>(g, host);
+  }
+}
+
+int psl_get_shifts(const psl_grid* g, int* s) {
+  PSL_CHECK(g && s, PSL_ERR_INVALID, "psl_get_shifts: null argument");
+  for (int q = 0; q < 27; ++q) s[q] = (int)g->shift[q];
+  return PSL_OK;
+}
+
+int psl_set_shifts(psl_grid* g, const int* s) {
+  PSL_CHECK(g && s, PSL_ERR_INVALID, "psl_set_shifts: null argument");
+  for (int q = 0; q < 27; ++q)
+    PSL_CHECK(s[q] >= 0 && (uint32_t)s[q] < g->n, PSL_ERR_INVALID, "psl_set_shifts: shift outside [0, N)");
+  for (int q = 0; q < 27; ++q) g->shift[q] = (uint32_t)s[q];
+  return PSL_OK;
+}
+
+int psl_synchronize(psl_grid* g) {
+  PSL_CHECK(g, PSL_ERR_INVALID, "psl_synchronize: null grid");
+  DeviceGuard dg(g->device);
+  PSL_CUDA(cudaStreamSynchronize(g->stream));
+  return PSL_OK;
+}
+
+int psl_check_health(psl_grid* g, unsigned int* flags) {
+  PSL_CHECK(g && flags, PSL_ERR_INVALID, "psl_check_health: null argument");
+  DeviceGuard dg(g->device);
+  PSL_CUDA(cudaMemcpyAsync(flags, g->health, sizeof(unsigned int), cudaMemcpyDeviceToHost, g->stream));
+  PSL_CUDA(cudaMemsetAsync(g->health, 0, sizeof(unsigned int), g->stream));
+  PSL_CUDA(cudaStreamSynchronize(g->stream));
+  return PSL_OK;
+}
+
+int psl_debug_cells(int op, int a0, float* host_f, const float* host_args, int count) {
+  PSL_CHECK(host_f && host_args && count > 0, PSL_ERR_INVALID, "psl_debug_cells: bad argument");
+  int ndev = 0;
+  PSL_CUDA(cudaGetDeviceCount(&ndev));
+  PSL_CHECK(ndev > 0, PSL_ERR_CUDA, "psl_debug_cells: no CUDA device");
+  float *df = nullptr, *da = nullptr;
+  PSL_CUDA(cudaMalloc(&df, (size_t)count * 27 * sizeof(float)));
+  cudaError_t e = cudaMalloc(&da, (size_t)count * 4 * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpy(df, host_f, (size_t)count * 27 * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(da, host_args, (size_t)count * 4 * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    debug_cell_kernel<<<blocks_for(count, 64), 64>>>(op, a0, df, da, count);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(host_f, df, (size_t)count * 27 * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(df);
+  if (da) cudaFree(da);
+  if (e != cudaSuccess) return fail(PSL_ERR_CUDA, std::string("psl_debug_cells: ") + cudaGetErrorString(e));
+  return PSL_OK;
+}
+

@@ -1,0 +1,489 @@
+// CUDA kernels of the per-step lattice update (sm_100a).
+//
+// Data layout in HBM (per grid): populations as 27 rows of `stride` elements (structure of
+// arrays, the reference's fArray[27][N], include/types.h:42-45), row q starting 128-byte
+// aligned; a one-byte marker per cell; 27 periodic-shift offsets kept on the host and
+// passed as kernel parameters.  Population q of cell c lives at row q, address
+// (c + shift_q) mod N (applyStreaming.h:33-41); streaming only changes the 27 offsets.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "psl_bc_generated.cuh"
+#include "psl_collision.cuh"
+#include "psl_hooks.cuh"
+#include "psl_lattice.cuh"
+#include "psl_storage.cuh"
+
+namespace psl {
+
+constexpr int kStepThreads = 128;
+
+// Shifted address of population q of `cell` (getShiftedIndex, applyStreaming.h:33-41).
+// cell < n and shift < n, so one conditional subtraction wraps it.
+__device__ __forceinline__ uint32_t shifted(uint32_t cell, uint32_t shift, uint32_t n) {
+  const uint32_t a = cell + shift;
+  return a >= n ? a - n : a;
+}
+
+template <typename S>
+struct GridView {
+  typename S::type* fq[27];  // row q of the population array
+  uint32_t shift[27];
+  uint32_t n;                // cells (the periodic-shift modulus)
+};
+
+// ------------------------------------------------------------------------------------------
+// fused per-cell update: gather -> bounce-back | (boundary condition) -> collision -> scatter
+// ------------------------------------------------------------------------------------------
+template <typename S>
+struct StepParams {
+  GridView<S> g;
+  const uint8_t* marker;
+  const float4* given;   // per-cell (rho, ux, uy, uz) for boundary cells, or null
+  float4 given_uniform;  // used when `given` is null
+  Relaxation rx;
+  unsigned int* health;  // bit 0 set when a collided cell's density is not finite/positive
+};
+
+// The boundary branch runs for ~2% of cells; keeping it out of line keeps the hot path's
+// instruction footprint small.  (applyLocalCellUpdate.h:41-67)
+__device__ __noinline__ void apply_boundary(uint8_t m, float (&f)[27], float4 given) {
+  const int kind = marker_kind(m), normal = marker_normal(m);
+  float rho = given.x, ux = given.y, uy = given.z, uz = given.w;
+  if (kind == kMirror) {
+    bc::mirror(normal, f);
+    return;
+  }
+  if (kind == kGivenRho) bc::restore_u(normal, f, rho, ux, uy, uz);
+  else if (kind == kGivenU) bc::restore_rho(normal, f, rho, ux, uy, uz);
+  else if (kind == kGivenNone) bc::restore_rho_u(normal, f, rho, ux, uy, uz);
+  bc::mbbc(normal, f, rho, ux, uy, uz);
+}
+
+template <typename S, int Q = 0>
+__device__ __forceinline__ void load_cell(const GridView<S>& g, uint32_t cell, float (&f)[27]) {
+  if constexpr (Q < 27) {
+    f[Q] = S::template load<Q>(g.fq[Q] + shifted(cell, g.shift[Q], g.n));
+    load_cell<S, Q + 1>(g, cell, f);
+  }
+}
+template <typename S, int Q = 0>
+__device__ __forceinline__ void store_cell(const GridView<S>& g, uint32_t cell, const float (&f)[27]) {
+  if constexpr (Q < 27) {
+    S::template store<Q>(g.fq[Q] + shifted(cell, g.shift[Q], g.n), f[Q]);
+    store_cell<S, Q + 1>(g, cell, f);
+  }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constant__ StepParams<S> p) {
+  const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
+  if (cell >= p.g.n) return;
+  const uint8_t m = p.marker[cell];
+  const int kind = marker_kind(m);
+  if (kind == kSkip) return;
+  float f[27];
+  load_cell<S>(p.g, cell, f);
+  if (kind == kSolid) {
+#pragma unroll
+    for (int q = 1; q < 27; q += 2) {
+      const float t = f[q];
+      f[q] = f[q + 1];
+      f[q + 1] = t;
+    }
+  } else {
+    if (kind != kFluid) apply_boundary(m, f, p.given ? p.given[cell] : p.given_uniform);
+    collide<false>(f, p.rx);
+    if (p.health) {
+      const float r = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6];
+      if (!(r > 0.f && r < 1.0e30f)) atomicOr(p.health, 1u);
+    }
+  }
+  store_cell<S>(p.g, cell, f);
+}
+
+// ------------------------------------------------------------------------------------------
+// set-up kernels (hooks)
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void cell_ijk(uint32_t cell, const InfoStruct& I, int& i, int& j, int& k) {
+  const uint32_t xy = (uint32_t)I.cellCountX * (uint32_t)I.cellCountY;
+  k = (int)(cell / xy);
+  const uint32_t r = cell - (uint32_t)k * xy;
+  j = (int)(r / (uint32_t)I.cellCountX);
+  i = (int)(r - (uint32_t)j * (uint32_t)I.cellCountX);
+}
+
+template <typename Case>
+__global__ void fill_markers_kernel(Case c, InfoStruct I, uint32_t n, uint8_t* marker, float4* given) {
+  const uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= n) return;
+  int i, j, k;
+  cell_ijk(cell, I, i, j, k);
+  MarkerStruct M;
+  c.getMarkers(i, j, k, M, I);
+  marker[cell] = encode_marker(i, j, k, M, I);
+  if (given) {
+    float rho = 1.f, ux = 0.f, uy = 0.f, uz = 0.f;
+    c.getGivenRhoUxUyUz(i, j, k, rho, ux, uy, uz, I);
+    given[cell] = make_float4(rho, ux, uy, uz);
+  }
+}
+
+// second-order equilibrium (include/cellFunctions.h:60-121)
+__device__ __forceinline__ void equilibrium(float rho, float ux, float uy, float uz, float (&fe)[27]) {
+  const float u2 = ux * ux + uy * uy + uz * uz;
+#pragma unroll
+  for (int q = 0; q < 27; ++q) {
+    const float cu = (float)cx(q) * ux + (float)cy(q) * uy + (float)cz(q) * uz;
+    fe[q] = rho * lattice_weight(q) * (1.f + 3.f * cu + 4.5f * cu * cu - 1.5f * u2);
+  }
+}
+
+template <typename S, typename Case>
+__global__ void fill_equilibrium_kernel(GridView<S> g, Case c, InfoStruct I) {
+  const uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= g.n) return;
+  int i, j, k;
+  cell_ijk(cell, I, i, j, k);
+  MarkerStruct M;
+  float rho = 1.f, ux = 0.f, uy = 0.f, uz = 0.f;
+  c.getInitialRhoUxUyUz(i, j, k, rho, ux, uy, uz, M, I);
+  float fe[27];
+  equilibrium(rho, ux, uy, uz, fe);
+  store_cell<S>(g, cell, fe);
+}
+
+// ------------------------------------------------------------------------------------------
+// periodic x / y fix-up after streaming (include/boundaryConditions/periodicXY.h:11-101):
+// the 9 populations with c_x > 0 of the left face come from the right face, those with
+// c_x < 0 of the right face from the left face (layers 0 and N-1 coincide).
+// ------------------------------------------------------------------------------------------
+template <typename S, int Axis>
+__global__ void periodic_kernel(GridView<S> g, int nx, int ny, int nz) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int na = Axis == 0 ? ny : nx;
+  if (t >= na * nz) return;
+  const int a = t % na, k = t / na;
+  uint32_t left, right;
+  if (Axis == 0) {
+    left = ((uint32_t)k * ny + a) * nx;
+    right = left + nx - 1;
+  } else {
+    left = ((uint32_t)k * ny) * nx + a;
+    right = ((uint32_t)k * ny + (ny - 1)) * nx + a;
+  }
+#pragma unroll
+  for (int q = 1; q < 27; ++q) {
+    const int c = Axis == 0 ? cx(q) : cy(q);
+    if (c > 0) {
+      g.fq[q][shifted(left, g.shift[q], g.n)] = g.fq[q][shifted(right, g.shift[q], g.n)];
+    } else if (c < 0) {
+      g.fq[q][shifted(right, g.shift[q], g.n)] = g.fq[q][shifted(left, g.shift[q], g.n)];
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// coarse <-> fine transfer as ONE kernel (include/gridRefinementFunctions.h:283-526)
+//
+// Phase 1 (restriction): every coarse cell on the surface of the box
+//   [iS+1, iE-2] x [jS+1, jE-2] x [kS+1, kE-2] gets the average of its 8 fine children,
+//   rescaled fine->coarse (writeToCoarseGridInterface; the reference's six face launches
+//   overlap on edges and corners with identical values, here each cell is written once).
+// Grid-wide barrier (cooperative launch; bounded spin, see grid_barrier).
+// Phase 2 (prolongation): every fine cell in the two outer layers of each active face gets
+//   the 7-point interpolation of the coarse field around its parent, rescaled
+//   coarse->fine (writeToFineGridInterface).  Ghost cells receive only the populations of
+//   the faces they belong to that stream inward (the union of those faces' 9-direction
+//   sets); other cells receive all 27.  The reference runs six face launches in sequence;
+//   since every launch computes the same value for a given fine cell, the union is the
+//   same final state.
+// ------------------------------------------------------------------------------------------
+struct CoarseFineParams {
+  GridView<StoreF32> c;
+  GridView<StoreF32> f;
+  int cnx, cny, cnz;
+  int iS, jS, kS, iE, jE, kE;
+  int fnx, fny, fnz;
+  const uint8_t* fine_marker;
+  int face_active;          // bit 2*axis: start face, bit 2*axis+1: end face
+  uint32_t n_ring;          // restriction work items
+  uint32_t n_shell;         // prolongation work items
+  unsigned int* barrier;    // zeroed before launch
+  unsigned int* error;      // bit 1: barrier gave up
+  unsigned int nblocks;
+};
+
+// direction sets streaming inward across each face (gridRefinementFunctions.h:441-446):
+// dir_mask(axis, +1) for a start face, dir_mask(axis, -1) for an end face
+constexpr uint32_t kAllDirs = (1u << 27) - 1;
+
+// Bounded grid-wide barrier for a cooperative launch: every block's thread 0 arrives once
+// and spins (with a limit) until all `nblocks` have arrived.  A timed-out wait sets an
+// error bit and returns, so the kernel always terminates.
+__device__ __forceinline__ void grid_barrier(unsigned int* counter, unsigned int nblocks, unsigned int* error) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(counter, 1u);
+    unsigned int spins = 0;
+    while (true) {
+      const unsigned int v = *((volatile unsigned int*)counter);
+      if (v >= nblocks) break;
+      if (++spins > (1u << 26)) {
+        atomicOr(error, 2u);
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void load_cell_cg(const GridView<StoreF32>& g, uint32_t cell, float (&f)[27]) {
+#pragma unroll
+  for (int q = 0; q < 27; ++q) f[q] = __ldcg(g.fq[q] + shifted(cell, g.shift[q], g.n));
+}
+
+__global__ void __launch_bounds__(256) coarse_fine_kernel(const __grid_constant__ CoarseFineParams p) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  // ---------------- phase 1: restriction ----------------
+  {
+    const int a = p.iE - p.iS - 2, b = p.jE - p.jS - 2, c = p.kE - p.kS - 2;  // ring box extents
+    const uint32_t faceK = 2u * a * b;
+    const uint32_t faceJ = 2u * a * (c - 2);
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < p.n_ring; t += stride) {
+      int ri, rj, rk;
+      if (t < faceK) {
+        const uint32_t layer = t / (a * b), r = t % (a * b);
+        rk = layer ? c - 1 : 0;
+        rj = r / a;
+        ri = r % a;
+      } else if (t < faceK + faceJ) {
+        const uint32_t u = t - faceK, layer = u / (a * (c - 2)), r = u % (a * (c - 2));
+        rj = layer ? b - 1 : 0;
+        rk = 1 + r / a;
+        ri = r % a;
+      } else {
+        const uint32_t u = t - faceK - faceJ, layer = u / ((b - 2) * (c - 2)), r = u % ((b - 2) * (c - 2));
+        ri = layer ? a - 1 : 0;
+        rj = 1 + r % (b - 2);
+        rk = 1 + r / (b - 2);
+      }
+      const int i = p.iS + 1 + ri, j = p.jS + 1 + rj, k = p.kS + 1 + rk;
+      const int fi = (i - p.iS) * 2, fj = (j - p.jS) * 2, fk = (k - p.kS) * 2;
+      float f[27];
+#pragma unroll
+      for (int q = 0; q < 27; ++q) f[q] = 0.f;
+#pragma unroll
+      for (int dk = 0; dk <= 1; ++dk)
+#pragma unroll
+        for (int dj = 0; dj <= 1; ++dj)
+#pragma unroll
+          for (int di = 0; di <= 1; ++di) {
+            const uint32_t fc = ((uint32_t)(fk + dk) * p.fny + (fj + dj)) * p.fnx + (fi + di);
+#pragma unroll
+            for (int q = 0; q < 27; ++q) f[q] = __fadd_rn(f[q], p.f.fq[q][shifted(fc, p.f.shift[q], p.f.n)]);
+          }
+#pragma unroll
+      for (int q = 0; q < 27; ++q) f[q] = f[q] * 0.125f;
+      rescale(f, false);
+      const uint32_t cc = ((uint32_t)k * p.cny + j) * p.cnx + i;
+#pragma unroll
+      for (int q = 0; q < 27; ++q) p.c.fq[q][shifted(cc, p.c.shift[q], p.c.n)] = f[q];
+    }
+  }
+  grid_barrier(p.barrier, p.nblocks, p.error);
+  // ---------------- phase 2: prolongation ----------------
+  const uint32_t kPos[3] = {dir_mask(0, 1), dir_mask(1, 1), dir_mask(2, 1)};
+  const uint32_t kNeg[3] = {dir_mask(0, -1), dir_mask(1, -1), dir_mask(2, -1)};
+  const int nx = p.fnx, ny = p.fny, nz = p.fnz;
+  const uint32_t zl = 4u * nx * ny, yl = 4u * nx * (nz - 4);
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < p.n_shell; t += stride) {
+    int i, j, k;
+    if (t < zl) {
+      const uint32_t layer = t / (nx * ny), r = t % (nx * ny);
+      k = layer < 2 ? layer : nz - 4 + layer;
+      j = r / nx;
+      i = r % nx;
+    } else if (t < zl + yl) {
+      const uint32_t u = t - zl, layer = u / (nx * (nz - 4)), r = u % (nx * (nz - 4));
+      j = layer < 2 ? layer : ny - 4 + layer;
+      k = 2 + r / nx;
+      i = r % nx;
+    } else {
+      const uint32_t u = t - zl - yl, layer = u / ((ny - 4) * (nz - 4)), r = u % ((ny - 4) * (nz - 4));
+      i = layer < 2 ? layer : nx - 4 + layer;
+      j = 2 + r % (ny - 4);
+      k = 2 + r / (ny - 4);
+    }
+    const uint32_t fcell = ((uint32_t)k * ny + j) * nx + i;
+    const uint8_t fm = p.fine_marker[fcell];
+    const bool ghost = marker_kind(fm) == kSkip && marker_normal(fm) == 1;
+    const int idx[3] = {i, j, k};
+    const int dim[3] = {nx, ny, nz};
+    uint32_t mask = 0;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      if ((p.face_active >> (2 * ax)) & 1)
+        if (idx[ax] < 2) mask |= ghost ? kPos[ax] : kAllDirs;
+      if ((p.face_active >> (2 * ax + 1)) & 1)
+        if (idx[ax] >= dim[ax] - 2) mask |= ghost ? kNeg[ax] : kAllDirs;
+    }
+    if (!mask) continue;
+    const int ic = i / 2 + p.iS, jc = j / 2 + p.jS, kc = k / 2 + p.kS;
+    const float d[3] = {(i & 1) ? 0.25f : -0.25f, (j & 1) ? 0.25f : -0.25f, (k & 1) ? 0.25f : -0.25f};
+    float f[27];
+    load_cell_cg(p.c, ((uint32_t)kc * p.cny + jc) * p.cnx + ic, f);
+    const int cidx[3] = {ic, jc, kc};
+    const int cdim[3] = {p.cnx, p.cny, p.cnz};
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      int plus = cidx[ax] + 1, minus = cidx[ax] - 1;
+      float inv = 0.5f;
+      if (plus >= cdim[ax]) { plus = cidx[ax]; inv = 1.f; }
+      if (minus < 0) { minus = 0; inv = 1.f; }
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        int nb[3] = {ic, jc, kc};
+        nb[ax] = side == 0 ? plus : minus;
+        const float w = (side == 0 ? inv : -inv) * d[ax];  // exact: powers of two
+        const uint32_t nc = ((uint32_t)nb[2] * p.cny + nb[1]) * p.cnx + nb[0];
+#pragma unroll
+        for (int q = 0; q < 27; ++q) f[q] = __fadd_rn(f[q], __ldcg(p.c.fq[q] + shifted(nc, p.c.shift[q], p.c.n)) * w);
+      }
+    }
+    rescale(f, true);
+#pragma unroll
+    for (int q = 0; q < 27; ++q)
+      if (mask & (1u << q)) p.f.fq[q][shifted(fcell, p.f.shift[q], p.f.n)] = f[q];
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// momentum-exchange force on the solid cells of a box, FP64
+// (getSphereDrag, flowAroundSphereMainSingle.cu:99-156; per cell rho*(u - u_bounced))
+// Deterministic: per-block partial sums, then one block sums them in block order.
+// ------------------------------------------------------------------------------------------
+template <typename S>
+__global__ void __launch_bounds__(256) force_partial_kernel(GridView<S> g, const uint8_t* marker, int nx, int ny,
+                                                            int i0, int j0, int k0, int si, int sj, int sk,
+                                                            double* partial) {
+  const uint32_t total = (uint32_t)si * sj * sk;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int i = i0 + (int)(t % si), j = j0 + (int)((t / si) % sj), k = k0 + (int)(t / (si * sj));
+    const uint32_t cell = ((uint32_t)k * ny + j) * nx + i;
+    if (marker_kind(marker[cell]) != kSolid) continue;
+    double rho = 0, jx = 0, jy = 0, jz = 0, bx = 0, by = 0, bz = 0;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+      const double v = (double)S::load_q(g.fq[q] + shifted(cell, g.shift[q], g.n), q);
+      rho += v;
+      jx += cx(q) * v;
+      jy += cy(q) * v;
+      jz += cz(q) * v;
+      // the bounced population of direction q sits in direction opposite(q)
+      bx -= cx(q) * v;
+      by -= cy(q) * v;
+      bz -= cz(q) * v;
+    }
+    acc[0] += rho * (jx / rho - bx / rho);
+    acc[1] += rho * (jy / rho - by / rho);
+    acc[2] += rho * (jz / rho - bz / rho);
+  }
+  __shared__ double red[3][256];
+  for (int c = 0; c < 3; ++c) red[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s)
+      for (int c = 0; c < 3; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int c = 0; c < 3; ++c) partial[blockIdx.x * 3 + c] = red[c][0];
+}
+
+__global__ void force_final_kernel(const double* partial, int nblocks, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s[3] = {0, 0, 0};
+    for (int b = 0; b < nblocks; ++b)
+      for (int c = 0; c < 3; ++c) s[c] += partial[b * 3 + c];
+    for (int c = 0; c < 3; ++c) out[c] = s[c];
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// logical-order gather / scatter (host I/O; population q of cell c at [q][c])
+// ------------------------------------------------------------------------------------------
+template <typename S>
+__global__ void gather_logical_kernel(GridView<S> g, int q, float* out) {
+  const uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= g.n) return;
+  out[cell] = S::load_q(g.fq[q] + shifted(cell, g.shift[q], g.n), q);
+}
+template <typename S>
+__global__ void scatter_logical_kernel(GridView<S> g, int q, const float* in) {
+  const uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= g.n) return;
+  S::store_q(g.fq[q] + shifted(cell, g.shift[q], g.n), in[cell], q);
+}
+
+// ------------------------------------------------------------------------------------------
+// single-cell entry points (unit-level parity of the device functions)
+// ------------------------------------------------------------------------------------------
+__global__ void debug_cell_kernel(int op, int a0, float* f, const float* args, int count) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  float v[27];
+  float* base = f + (size_t)t * 27;
+  for (int q = 0; q < 27; ++q) v[q] = base[q];
+  const float* a = args + (size_t)t * 4;
+  switch (op) {
+    case 0: {  // collision (a: nu, cs)
+      Relaxation rx;
+      rx.tau = 3.f * a[0] + 0.5f;
+      rx.tau2 = rx.tau * rx.tau;
+      rx.omega0 = 1.f / rx.tau;
+      rx.cs18 = 18.f * a[1];
+      collide<false>(v, rx);
+      break;
+    }
+    case 1: rescale(v, a0 != 0); break;
+    case 2: bc::mbbc(a0, v, a[0], a[1], a[2], a[3]); break;
+    case 3: {
+      float rho = a[0], ux = a[1], uy = a[2], uz = a[3];
+      bc::restore_rho(a0, v, rho, ux, uy, uz);
+      v[0] = rho;
+      break;
+    }
+    case 4: {
+      float rho = a[0], ux = a[1], uy = a[2], uz = a[3];
+      bc::restore_u(a0, v, rho, ux, uy, uz);
+      v[0] = ux; v[1] = uy; v[2] = uz;
+      break;
+    }
+    case 5: {
+      float rho = a[0], ux = a[1], uy = a[2], uz = a[3];
+      bc::restore_rho_u(a0, v, rho, ux, uy, uz);
+      v[0] = rho; v[1] = ux; v[2] = uy; v[3] = uz;
+      break;
+    }
+    case 6: bc::mirror(a0, v); break;
+    case 7: {  // forced collision (a: nu, cs, gx; gy=gz=a[3])
+      Relaxation rx;
+      rx.tau = 3.f * a[0] + 0.5f;
+      rx.tau2 = rx.tau * rx.tau;
+      rx.omega0 = 1.f / rx.tau;
+      rx.cs18 = 18.f * a[1];
+      collide<true>(v, rx, a[2], a[3], 0.f);
+      break;
+    }
+    default: break;
+  }
+  for (int q = 0; q < 27; ++q) base[q] = v[q];
+}
+
+}  // namespace psl

@@ -1,0 +1,58 @@
+// Population storage formats.  All arithmetic is FP32; only the bytes in HBM differ.
+//
+//   F32            f_q stored as is                       (216 B moved per cell update)
+//   F16 / BF16     f_q - w_q stored in 16 bits            (108 B per cell update)
+//
+// Storing the deviation from the lattice weight keeps the stored values small (|f - w|
+// is O(u) relative to w), so the 16-bit formats spend their mantissa on the part that
+// changes.  The north_star precision form.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "psl_lattice.cuh"
+
+namespace psl {
+
+enum StorageKind : int { kStoreF32 = 0, kStoreF16 = 1, kStoreBF16 = 2 };
+
+struct StoreF32 {
+  using type = float;
+  static constexpr int kind = kStoreF32;
+  template <int Q>
+  __device__ __forceinline__ static float load(const float* p) { return *p; }
+  template <int Q>
+  __device__ __forceinline__ static void store(float* p, float v) { *p = v; }
+  __device__ __forceinline__ static float load_q(const float* p, int) { return *p; }
+  __device__ __forceinline__ static void store_q(float* p, float v, int) { *p = v; }
+};
+
+struct StoreF16 {
+  using type = __half;
+  static constexpr int kind = kStoreF16;
+  template <int Q>
+  __device__ __forceinline__ static float load(const __half* p) { return __half2float(*p) + lattice_weight(Q); }
+  template <int Q>
+  __device__ __forceinline__ static void store(__half* p, float v) { *p = __float2half_rn(v - lattice_weight(Q)); }
+  __device__ __forceinline__ static float load_q(const __half* p, int q) { return __half2float(*p) + lattice_weight(q); }
+  __device__ __forceinline__ static void store_q(__half* p, float v, int q) { *p = __float2half_rn(v - lattice_weight(q)); }
+};
+
+struct StoreBF16 {
+  using type = __nv_bfloat16;
+  static constexpr int kind = kStoreBF16;
+  template <int Q>
+  __device__ __forceinline__ static float load(const __nv_bfloat16* p) { return __bfloat162float(*p) + lattice_weight(Q); }
+  template <int Q>
+  __device__ __forceinline__ static void store(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v - lattice_weight(Q)); }
+  __device__ __forceinline__ static float load_q(const __nv_bfloat16* p, int q) {
+    return __bfloat162float(*p) + lattice_weight(q);
+  }
+  __device__ __forceinline__ static void store_q(__nv_bfloat16* p, float v, int q) {
+    *p = __float2bfloat16_rn(v - lattice_weight(q));
+  }
+};
+
+inline size_t storage_bytes(int kind) { return kind == kStoreF32 ? 4 : 2; }
+
+}  // namespace psl

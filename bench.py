@@ -38,10 +38,12 @@ BYTES_PER_UPDATE = {"f32": 216, "f16": 108, "bf16": 108}
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
-    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="native", choices=["native", "reference"])
     p.add_argument("--config", type=int, default=2, choices=[1, 2])
+    p.add_argument("--scale", type=float, default=1.0,
+                   help="linear scale of the config-2 geometry (0.5: a 256x128x128 case for ncu captures)")
     p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-steps", type=int, default=2)
@@ -51,7 +53,7 @@ def parse():
 def workload(args):
     from periodicshiftlbm_b200.cases import config1, config2
 
-    return config2() if args.config == 2 else config1()
+    return config2(scale=args.scale) if args.config == 2 else config1()
 
 
 def dist_env():
@@ -62,50 +64,67 @@ def dist_env():
 # clocks sampled during the timed region
 # ------------------------------------------------------------------------------------------
 class ClockSampler:
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """Samples the SM clock and the clock-event (throttle) reasons through NVML every
+    `period_s` in a background thread while the timed region runs (read-only queries)."""
 
-    def __init__(self, gpu_index: int):
+    REASONS = {
+        "hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+        "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+        "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+        "sw_power_cap": "nvmlClocksEventReasonSwPowerCap",
+        "hw_power_brake_slowdown": "nvmlClocksEventReasonHwPowerBrakeSlowdown",
+    }
+
+    def __init__(self, gpu_index: int, period_s: float = 0.005):
         self.gpu = gpu_index
-        self.proc = None
-        self.path = os.path.join(REPO, "gpurun_out", f"clocks_rank{gpu_index}.csv") if os.path.isdir(
-            os.path.join(REPO, "gpurun_out")) else f"/tmp/psl_clocks_{os.getpid()}.csv"
+        self.period = period_s
+        self.samples = []
+        self.thread = None
 
     def start(self):
+        import threading
+
         try:
-            self.fh = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
-                                         stderr=subprocess.DEVNULL)
+            import pynvml
+
+            pynvml.nvmlInit()
+            visible = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(visible.split(",")[self.gpu]) if visible else self.gpu
+            self.nvml = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
         except Exception:
-            self.proc = None
+            self.nvml = None
+            return
+        self.stop_flag = threading.Event()
+
+        def loop():
+            nv = self.nvml
+            while not self.stop_flag.is_set():
+                try:
+                    mhz = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                    reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                    self.samples.append((mhz, reasons))
+                except Exception:
+                    pass
+                self.stop_flag.wait(self.period)
+
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
 
     def stop(self):
-        if not self.proc:
+        if not self.thread:
             return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        self.fh.close()
-        rows = []
-        for line in open(self.path):
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                rows.append((float(parts[1]), float(parts[2]), parts[4:]))
-            except ValueError:
-                continue
-        if not rows:
+        self.stop_flag.set()
+        self.thread.join(timeout=2)
+        if not self.samples:
             return None
-        loaded = [r for r in rows if r[0] > 0.5 * r[1]] or rows
-        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in loaded for i in range(1, 5) if "Active" in r[2][i]})
-        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": max(r[1] for r in rows),
-                "reasons": reasons, "samples": len(rows)}
+        nv = self.nvml
+        mhz = [m for m, _ in self.samples]
+        active = sorted({name for name, attr in self.REASONS.items()
+                         for _, r in self.samples if hasattr(nv, attr) and r & getattr(nv, attr)})
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": self.max_mhz, "reasons": active,
+                "samples": len(self.samples), "source": "nvml"}
 
 
 # ------------------------------------------------------------------------------------------
@@ -224,18 +243,22 @@ def run_native(args):
     achieved = coarse_bytes / (coarse_ms * 1e-3) / 1e9
 
     # ---- end to end through the public API with host buffers ----
-    host_state = [np.ascontiguousarray(g.fArray) for g in grids]
-    pinned = [torch.from_numpy(h).pin_memory() for h in host_state]
+    pinned_in = [torch.empty((27, g.cellCount), dtype=torch.float32).pin_memory() for g in grids]
+    pinned_out = [torch.empty((27, g.cellCount), dtype=torch.float32).pin_memory() for g in grids]
+    for g, h in zip(grids, pinned_in):
+        g.read_populations(h.numpy())
+    host_state = [h.numpy() for h in pinned_in]
     torch.cuda.synchronize()
     barrier()
     e0 = time.perf_counter()
-    for g, h in zip(grids, pinned):
-        g.fArray = h.numpy()
+    for g, h in zip(grids, pinned_in):
+        g.write_populations(h.numpy())
     drags = []
     for _ in range(args.steps):
         update(0, False)
         drags.append(float(getSphereForce(grids[-1], case)[0]))
-    out_state = [g.fArray for g in grids]
+    for g, h in zip(grids, pinned_out):
+        g.read_populations(h.numpy())
     torch.cuda.synchronize()
     e_s = time.perf_counter() - e0
     if world > 1:

@@ -76,10 +76,16 @@ def config1(**kw) -> SphereConfig:
     return replace(c, **kw)
 
 
-def config2(**kw) -> SphereConfig:
-    c = SphereConfig(name="sphere_512x256x256_re1e5_refined", nx=512, ny=256, nz=256, sphere=(128.0, 128.0, 128.0),
-                     radius=24.0, u_in=0.05, nu=0.05 * 48 / 1e5, smagorinsky=0.1,
-                     refine=((80, 80, 80), (208, 176, 176)))
+def config2(scale: float = 1.0, **kw) -> SphereConfig:
+    """`scale` shrinks every length (grid, sphere, block) for small profiling runs; the
+    Reynolds number is kept (nu scales with the diameter)."""
+    def s(v):
+        return int(round(v * scale))
+
+    name = "sphere_512x256x256_re1e5_refined" if scale == 1.0 else f"sphere_{s(512)}x{s(256)}x{s(256)}_re1e5_refined"
+    c = SphereConfig(name=name, nx=s(512), ny=s(256), nz=s(256), sphere=(128.0 * scale,) * 3,
+                     radius=24.0 * scale, u_in=0.05, nu=0.05 * 48 * scale / 1e5, smagorinsky=0.1,
+                     refine=((s(80), s(80), s(80)), (s(208), s(176), s(176))))
     return replace(c, **kw)
 
 

@@ -469,13 +469,14 @@ static int gather(psl_grid* g, float* host) {
   PSL_CUDA(cudaMalloc(&tmp, (size_t)g->n * sizeof(float)));
   cudaError_t e = cudaSuccess;
   const GridView<S> v = view<S>(g);
+  // one staging row; stream order serialises each row's gather after the previous copy
   for (int q = 0; q < 27 && e == cudaSuccess; ++q) {
     gather_logical_kernel<S><<<blocks_for(g->n, 256), 256, 0, g->stream>>>(v, q, tmp);
     e = cudaGetLastError();
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(host + (size_t)q * g->n, tmp, (size_t)g->n * sizeof(float), cudaMemcpyDeviceToHost, g->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
   }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
   cudaFree(tmp);
   if (e != cudaSuccess) return fail(PSL_ERR_CUDA, std::string("psl_get_populations: ") + cudaGetErrorString(e));
   return PSL_OK;
@@ -493,8 +494,8 @@ static int scatter(psl_grid* g, const float* host) {
       scatter_logical_kernel<S><<<blocks_for(g->n, 256), 256, 0, g->stream>>>(v, q, tmp);
       e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
   }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
   cudaFree(tmp);
   if (e != cudaSuccess) return fail(PSL_ERR_CUDA, std::string("psl_set_populations: ") + cudaGetErrorString(e));
   return PSL_OK;

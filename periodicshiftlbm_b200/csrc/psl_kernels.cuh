@@ -242,9 +242,12 @@ __device__ __forceinline__ void grid_barrier(unsigned int* counter, unsigned int
   __syncthreads();
 }
 
-__device__ __forceinline__ void load_cell_cg(const GridView<StoreF32>& g, uint32_t cell, float (&f)[27]) {
+// Coarse reads after the grid barrier use ordinary (L1-cached) loads: no SM read a coarse
+// line before the barrier in this launch, and L1 starts empty for every launch, so no
+// stale copy of a restricted ring cell can be hit.
+__device__ __forceinline__ void load_cell_plain(const GridView<StoreF32>& g, uint32_t cell, float (&f)[27]) {
 #pragma unroll
-  for (int q = 0; q < 27; ++q) f[q] = __ldcg(g.fq[q] + shifted(cell, g.shift[q], g.n));
+  for (int q = 0; q < 27; ++q) f[q] = g.fq[q][shifted(cell, g.shift[q], g.n)];
 }
 
 __global__ void __launch_bounds__(256) coarse_fine_kernel(const __grid_constant__ CoarseFineParams p) {
@@ -336,7 +339,7 @@ __global__ void __launch_bounds__(256) coarse_fine_kernel(const __grid_constant_
     const int ic = i / 2 + p.iS, jc = j / 2 + p.jS, kc = k / 2 + p.kS;
     const float d[3] = {(i & 1) ? 0.25f : -0.25f, (j & 1) ? 0.25f : -0.25f, (k & 1) ? 0.25f : -0.25f};
     float f[27];
-    load_cell_cg(p.c, ((uint32_t)kc * p.cny + jc) * p.cnx + ic, f);
+    load_cell_plain(p.c, ((uint32_t)kc * p.cny + jc) * p.cnx + ic, f);
     const int cidx[3] = {ic, jc, kc};
     const int cdim[3] = {p.cnx, p.cny, p.cnz};
 #pragma unroll
@@ -352,7 +355,7 @@ __global__ void __launch_bounds__(256) coarse_fine_kernel(const __grid_constant_
         const float w = (side == 0 ? inv : -inv) * d[ax];  // exact: powers of two
         const uint32_t nc = ((uint32_t)nb[2] * p.cny + nb[1]) * p.cnx + nb[0];
 #pragma unroll
-        for (int q = 0; q < 27; ++q) f[q] = __fadd_rn(f[q], __ldcg(p.c.fq[q] + shifted(nc, p.c.shift[q], p.c.n)) * w);
+        for (int q = 0; q < 27; ++q) f[q] = __fadd_rn(f[q], p.c.fq[q][shifted(nc, p.c.shift[q], p.c.n)] * w);
       }
     }
     rescale(f, true);

@@ -151,6 +151,17 @@ class GridStruct:
         f = np.ascontiguousarray(f, dtype=np.float32).reshape(27, self.cellCount)
         call("psl_set_populations", self._h, f.ctypes.data)
 
+    def read_populations(self, out: np.ndarray) -> np.ndarray:
+        """fArray into a caller-provided float32 [27][N] buffer (e.g. pinned host memory)."""
+        assert out.dtype == np.float32 and out.size == 27 * self.cellCount and out.flags.c_contiguous
+        call("psl_get_populations", self._h, out.ctypes.data)
+        return out
+
+    def write_populations(self, src: np.ndarray):
+        """Set fArray from a caller-provided float32 [27][N] buffer."""
+        assert src.dtype == np.float32 and src.size == 27 * self.cellCount and src.flags.c_contiguous
+        call("psl_set_populations", self._h, src.ctypes.data)
+
     @property
     def shifter(self) -> np.ndarray:
         out = np.zeros(27, dtype=np.int32)

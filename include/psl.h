@@ -121,6 +121,26 @@ int psl_update_grid(psl_grid** grids, int levels, int level);
  * drag (x), force[1..2] the y and z components. */
 int psl_sphere_force(psl_grid* grid, const psl_sphere_case* sc, double* force3);
 
+/* Momentum-exchange force over the solid cells of the box [box_lo3, box_hi3), FP64, on
+ * caller-owned buffers, allocating no device memory.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc when they need the force: step loops running
+ * inside CUDA stream capture, applications whose device memory belongs to another
+ * allocator's pool or a fixed budget, and loops that must not block on an allocation.
+ *   populations  device pointer to 27 FP32 rows of row_stride elements (row q holds
+ *                population q at the periodic-shift address (cell + shifts27[q]) mod N)
+ *   shifts27     host array, each in [0, cell_count); cell_count = nx*ny*nz
+ *   markers      device marker bytes (cells of kind PSL_CELL_SOLID are summed)
+ *   force3       device pointer; receives (Fx, Fy, Fz) in lattice units
+ * Work is queued on cuda_stream (NULL = legacy default stream); nothing is synchronised.
+ * Partial sums live in a fixed 24.6 KB array inside the library, held by every GPU that
+ * loads it until exit; the box may hold at most 4,194,304 cells (else PSL_ERR_INVALID).
+ * The first call on a device looks that array up (cudaGetSymbolAddress) with the device
+ * current: make it before any stream capture.  All calls share the array, so calls whose
+ * kernels overlap on the GPU (different streams) race; order them on one stream. */
+int psl_momentum_exchange_force_noalloc(const float* populations, long long row_stride, const int* shifts27,
+                                        long long cell_count, const uint8_t* markers, int nx, int ny, int nz,
+                                        const int* box_lo3, const int* box_hi3, double* force3, void* cuda_stream);
+
 /* ---- data movement ---- */
 /* Populations in logical order: host[q * N + cell] = f_q of `cell` (FP32 for every storage). */
 int psl_get_populations(psl_grid* grid, float* host);

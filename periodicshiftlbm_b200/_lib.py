@@ -73,6 +73,10 @@ _SIGNATURES = {
     "psl_apply_coarse_fine_grid_communication": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_update_grid": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int]),
     "psl_sphere_force": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PslSphereCase), ctypes.c_void_p]),
+    "psl_momentum_exchange_force_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p,
+                                                           ctypes.c_longlong, ctypes.c_void_p, ctypes.c_int,
+                                                           ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                           ctypes.c_void_p, ctypes.c_void_p]),
     "psl_get_populations": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_set_populations": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_get_shifts": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),

@@ -24,6 +24,9 @@ static int fail(int code, const std::string& msg) {
   return code;
 }
 
+// For the library's other translation units (psl_noalloc.cu).
+__attribute__((visibility("hidden"))) void psl_detail_set_last_error(const std::string& msg) { g_last_error = msg; }
+
 #define PSL_CUDA(expr)                                                                                 \
   do {                                                                                                 \
     cudaError_t e_ = (expr);                                                                           \

@@ -48,7 +48,7 @@ struct StepParams {
 
 // The boundary branch runs for ~2% of cells; keeping it out of line keeps the hot path's
 // instruction footprint small.  (applyLocalCellUpdate.h:41-67)
-__device__ __noinline__ void apply_boundary(uint8_t m, float (&f)[27], float4 given) {
+static __device__ __noinline__ void apply_boundary(uint8_t m, float (&f)[27], float4 given) {
   const int kind = marker_kind(m), normal = marker_normal(m);
   float rho = given.x, ux = given.y, uy = given.z, uz = given.w;
   if (kind == kMirror) {
@@ -250,7 +250,7 @@ __device__ __forceinline__ void load_cell_plain(const GridView<StoreF32>& g, uin
   for (int q = 0; q < 27; ++q) f[q] = g.fq[q][shifted(cell, g.shift[q], g.n)];
 }
 
-__global__ void __launch_bounds__(256) coarse_fine_kernel(const __grid_constant__ CoarseFineParams p) {
+static __global__ void __launch_bounds__(256) coarse_fine_kernel(const __grid_constant__ CoarseFineParams p) {
   const uint32_t stride = gridDim.x * blockDim.x;
   // ---------------- phase 1: restriction ----------------
   {
@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(256) force_partial_kernel(GridView<S> g, const
     for (int c = 0; c < 3; ++c) partial[blockIdx.x * 3 + c] = red[c][0];
 }
 
-__global__ void force_final_kernel(const double* partial, int nblocks, double* out) {
+static __global__ void force_final_kernel(const double* partial, int nblocks, double* out) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     double s[3] = {0, 0, 0};
     for (int b = 0; b < nblocks; ++b)
@@ -437,7 +437,7 @@ __global__ void scatter_logical_kernel(GridView<S> g, int q, const float* in) {
 // ------------------------------------------------------------------------------------------
 // single-cell entry points (unit-level parity of the device functions)
 // ------------------------------------------------------------------------------------------
-__global__ void debug_cell_kernel(int op, int a0, float* f, const float* args, int count) {
+static __global__ void debug_cell_kernel(int op, int a0, float* f, const float* args, int count) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
   float v[27];

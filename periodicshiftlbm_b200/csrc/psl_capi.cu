@@ -5,12 +5,14 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "psl.h"
 #include "psl_kernels.cuh"
+#include "psl_step_tiled.cuh"
 
 using namespace psl;
 
@@ -70,6 +72,7 @@ struct psl_grid {
   unsigned int* health = nullptr;   // [0] health bits, [1] barrier counter
   double* scratch = nullptr;        // force partials (kForceBlocks x 3) + result (3)
   int device = 0;
+  bool tiled = false;               // bulk-copy tiled update kernel (N % 128 == 0)
 };
 
 static constexpr int kForceBlocks = 512;
@@ -155,6 +158,10 @@ int psl_grid_create(const psl_info* info, int storage, psl_grid** out) {
   g->n = (uint32_t)n;
   g->storage = storage;
   g->stride = ((size_t)n + 63) / 64 * 64;
+  // PSL_STEP_KERNEL=tiled selects the bulk-copy tiled update kernel where it applies
+  // (N % 128 == 0); the default is the one-thread-per-cell kernel.
+  const char* kernel_choice = getenv("PSL_STEP_KERNEL");
+  g->tiled = kernel_choice && std::string(kernel_choice) == "tiled";
   cudaGetDevice(&g->device);
   const size_t bytes = 27 * g->stride * storage_bytes(storage);
   cudaError_t e = cudaMalloc(&g->f, bytes);
@@ -324,7 +331,19 @@ static void launch_step(psl_grid* g) {
   p.given_uniform = g->given_uniform;
   p.rx = relaxation(g);
   p.health = g->health;
-  step_kernel<S><<<blocks_for(g->n, kStepThreads), kStepThreads, 0, g->stream>>>(p);
+  p.ri.base = static_cast<typename S::type*>(g->f);
+  p.ri.n = g->n;
+  for (int q = 0; q < 27; ++q) {
+    p.ri.off[q] = (uint32_t)((size_t)q * g->stride + g->shift[q]);
+    p.ri.lim[q] = g->n - g->shift[q];
+  }
+  const bool row_index = 27 * g->stride + g->n < (1ull << 32);
+  if (g->tiled && g->n % kTile == 0)
+    step_tiled_kernel<S><<<g->n / kTile, kTile, 0, g->stream>>>(p);
+  else if (row_index)
+    step_kernel<S, true><<<blocks_for(g->n, kStepThreads), kStepThreads, 0, g->stream>>>(p);
+  else
+    step_kernel<S, false><<<blocks_for(g->n, kStepThreads), kStepThreads, 0, g->stream>>>(p);
 }
 
 int psl_apply_local_cell_update(psl_grid* g) {
@@ -402,13 +421,13 @@ int psl_apply_coarse_fine_grid_communication(psl_grid* c, psl_grid* f) {
   p.error = c->health;
   int sms = 0, per_sm = 0;
   PSL_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-  PSL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_fine_kernel, 256, 0));
+  PSL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_fine_kernel, kCoarseFineThreads, 0));
   PSL_CHECK(per_sm > 0, PSL_ERR_CUDA, "coarse/fine: kernel cannot be resident");
-  const unsigned int want = blocks_for(std::max(p.n_ring, p.n_shell), 256);
+  const unsigned int want = blocks_for(std::max(p.n_ring, p.n_shell), kCoarseFineThreads);
   p.nblocks = std::min<unsigned int>((unsigned int)(sms * per_sm), std::max(1u, want));
   PSL_CUDA(cudaMemsetAsync(p.barrier, 0, sizeof(unsigned int), c->stream));
   void* args[] = {&p};
-  PSL_CUDA(cudaLaunchCooperativeKernel((const void*)coarse_fine_kernel, dim3(p.nblocks), dim3(256), args, 0, c->stream));
+  PSL_CUDA(cudaLaunchCooperativeKernel((const void*)coarse_fine_kernel, dim3(p.nblocks), dim3(kCoarseFineThreads), args, 0, c->stream));
   return PSL_OK;
 }
 

@@ -36,9 +36,23 @@ struct GridView {
 // ------------------------------------------------------------------------------------------
 // fused per-cell update: gather -> bounce-back | (boundary condition) -> collision -> scatter
 // ------------------------------------------------------------------------------------------
+// Row addressing for the update kernel: one base pointer and 32-bit per-population
+// offsets.  Population q of `cell` lives at base[off_q + cell] while cell < lim_q, else at
+// base[off_q + cell - N], with off_q = q*stride + shift_q and lim_q = N - shift_q.  32-bit
+// kernel parameters serve as constant-bank operands, so no per-population 64-bit pointer
+// has to be fetched; usable while 27*stride + N < 2^32.
+template <typename S>
+struct RowIndex {
+  typename S::type* base;
+  uint32_t off[27];
+  uint32_t lim[27];
+  uint32_t n;
+};
+
 template <typename S>
 struct StepParams {
   GridView<S> g;
+  RowIndex<S> ri;
   const uint8_t* marker;
   const float4* given;   // per-cell (rho, ux, uy, uz) for boundary cells, or null
   float4 given_uniform;  // used when `given` is null
@@ -76,7 +90,26 @@ __device__ __forceinline__ void store_cell(const GridView<S>& g, uint32_t cell, 
   }
 }
 
-template <typename S>
+template <typename S, int Q = 0>
+__device__ __forceinline__ void load_cell_ri(const RowIndex<S>& r, uint32_t cell, float (&f)[27]) {
+  if constexpr (Q < 27) {
+    uint32_t i = cell + r.off[Q];
+    if (cell >= r.lim[Q]) i -= r.n;
+    f[Q] = S::template load_once<Q>(r.base + i);
+    load_cell_ri<S, Q + 1>(r, cell, f);
+  }
+}
+template <typename S, int Q = 0>
+__device__ __forceinline__ void store_cell_ri(const RowIndex<S>& r, uint32_t cell, const float (&f)[27]) {
+  if constexpr (Q < 27) {
+    uint32_t i = cell + r.off[Q];
+    if (cell >= r.lim[Q]) i -= r.n;
+    S::template store_once<Q>(r.base + i, f[Q]);
+    store_cell_ri<S, Q + 1>(r, cell, f);
+  }
+}
+
+template <typename S, bool kRowIndex>
 __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constant__ StepParams<S> p) {
   const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
   if (cell >= p.g.n) return;
@@ -84,7 +117,8 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constan
   const int kind = marker_kind(m);
   if (kind == kSkip) return;
   float f[27];
-  load_cell<S>(p.g, cell, f);
+  if constexpr (kRowIndex) load_cell_ri<S>(p.ri, cell, f);
+  else load_cell<S>(p.g, cell, f);
   if (kind == kSolid) {
 #pragma unroll
     for (int q = 1; q < 27; q += 2) {
@@ -100,8 +134,10 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constan
       if (!(r > 0.f && r < 1.0e30f)) atomicOr(p.health, 1u);
     }
   }
-  store_cell<S>(p.g, cell, f);
+  if constexpr (kRowIndex) store_cell_ri<S>(p.ri, cell, f);
+  else store_cell<S>(p.g, cell, f);
 }
+
 
 // ------------------------------------------------------------------------------------------
 // set-up kernels (hooks)
@@ -250,14 +286,22 @@ __device__ __forceinline__ void load_cell_plain(const GridView<StoreF32>& g, uin
   for (int q = 0; q < 27; ++q) f[q] = g.fq[q][shifted(cell, g.shift[q], g.n)];
 }
 
-static __global__ void __launch_bounds__(256) coarse_fine_kernel(const __grid_constant__ CoarseFineParams p) {
-  const uint32_t stride = gridDim.x * blockDim.x;
+// Work items are dealt out in warp-sized chunks, consecutive chunks to consecutive blocks,
+// so both phases spread over every SM while each warp still touches consecutive cells.
+#define PSL_FOR_EACH_ITEM(t, count)                                                                        \
+  for (uint32_t chunk_ = blockIdx.x + gridDim.x * (threadIdx.x >> 5); chunk_ * 32u < (count);            \
+       chunk_ += gridDim.x * (blockDim.x >> 5))                                                            \
+    for (uint32_t t = chunk_ * 32u + (threadIdx.x & 31u); t < (count); t = (count))
+
+constexpr int kCoarseFineThreads = 128;
+
+static __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const __grid_constant__ CoarseFineParams p) {
   // ---------------- phase 1: restriction ----------------
   {
     const int a = p.iE - p.iS - 2, b = p.jE - p.jS - 2, c = p.kE - p.kS - 2;  // ring box extents
     const uint32_t faceK = 2u * a * b;
     const uint32_t faceJ = 2u * a * (c - 2);
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < p.n_ring; t += stride) {
+    PSL_FOR_EACH_ITEM(t, p.n_ring) {
       int ri, rj, rk;
       if (t < faceK) {
         const uint32_t layer = t / (a * b), r = t % (a * b);
@@ -304,7 +348,7 @@ static __global__ void __launch_bounds__(256) coarse_fine_kernel(const __grid_co
   const uint32_t kNeg[3] = {dir_mask(0, -1), dir_mask(1, -1), dir_mask(2, -1)};
   const int nx = p.fnx, ny = p.fny, nz = p.fnz;
   const uint32_t zl = 4u * nx * ny, yl = 4u * nx * (nz - 4);
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < p.n_shell; t += stride) {
+  PSL_FOR_EACH_ITEM(t, p.n_shell) {
     int i, j, k;
     if (t < zl) {
       const uint32_t layer = t / (nx * ny), r = t % (nx * ny);

@@ -25,6 +25,12 @@ struct StoreF32 {
   __device__ __forceinline__ static void store(float* p, float v) { *p = v; }
   __device__ __forceinline__ static float load_q(const float* p, int) { return *p; }
   __device__ __forceinline__ static void store_q(float* p, float v, int) { *p = v; }
+  // Update-kernel forms: each element is read once by its owning cell (read-only path)
+  // and then overwritten by it (evict-first store).
+  template <int Q>
+  __device__ __forceinline__ static float load_once(const float* p) { return __ldg(p); }
+  template <int Q>
+  __device__ __forceinline__ static void store_once(float* p, float v) { __stcs(p, v); }
 };
 
 struct StoreF16 {
@@ -36,6 +42,12 @@ struct StoreF16 {
   __device__ __forceinline__ static void store(__half* p, float v) { *p = __float2half_rn(v - lattice_weight(Q)); }
   __device__ __forceinline__ static float load_q(const __half* p, int q) { return __half2float(*p) + lattice_weight(q); }
   __device__ __forceinline__ static void store_q(__half* p, float v, int q) { *p = __float2half_rn(v - lattice_weight(q)); }
+  template <int Q>
+  __device__ __forceinline__ static float load_once(const __half* p) { return __half2float(__ldg(p)) + lattice_weight(Q); }
+  template <int Q>
+  __device__ __forceinline__ static void store_once(__half* p, float v) {
+    __stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(__float2half_rn(v - lattice_weight(Q))));
+  }
 };
 
 struct StoreBF16 {
@@ -50,6 +62,14 @@ struct StoreBF16 {
   }
   __device__ __forceinline__ static void store_q(__nv_bfloat16* p, float v, int q) {
     *p = __float2bfloat16_rn(v - lattice_weight(q));
+  }
+  template <int Q>
+  __device__ __forceinline__ static float load_once(const __nv_bfloat16* p) {
+    return __bfloat162float(__ldg(p)) + lattice_weight(Q);
+  }
+  template <int Q>
+  __device__ __forceinline__ static void store_once(__nv_bfloat16* p, float v) {
+    __stcs(reinterpret_cast<unsigned short*>(p), __bfloat16_as_ushort(__float2bfloat16_rn(v - lattice_weight(Q))));
   }
 };
 

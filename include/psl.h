@@ -36,10 +36,12 @@ extern "C" {
 
 typedef struct psl_grid psl_grid;
 
-/* Population storage in HBM.  Arithmetic is FP32 in every form. */
+/* Population storage in HBM.  Arithmetic is FP32 in the three production forms. */
 #define PSL_STORAGE_F32 0       /* f_q as float (216 B moved per cell update) */
 #define PSL_STORAGE_F16_SHIFTED 1  /* f_q - w_q as IEEE half (108 B per cell update) */
 #define PSL_STORAGE_BF16_SHIFTED 2 /* f_q - w_q as bfloat16 (108 B per cell update) */
+#define PSL_STORAGE_F64 3       /* f_q as double with FP64 arithmetic: the FP64 oracle runs
+                                   that the reduced-precision forms are measured against */
 
 /* Per-grid metadata; mirrors InfoStruct (include/types.h:73-75). */
 typedef struct psl_info {
@@ -144,6 +146,11 @@ int psl_momentum_exchange_force_noalloc(const float* populations, long long row_
 /* ---- data movement ---- */
 /* Populations in logical order: host[q * N + cell] = f_q of `cell` (FP32 for every storage). */
 int psl_get_populations(psl_grid* grid, float* host);
+/* Macroscopic fields in logical order, summed in FP64 from the stored populations
+ * (getRhoUxUyUz, cellFunctions.h:135-155): host[0*N + cell] = rho, host[1*N + cell] = ux,
+ * host[2*N + cell] = uy, host[3*N + cell] = uz.  No reference counterpart as one call: the
+ * reference's exporters evaluate getRhoUxUyUz per cell on the host. */
+int psl_get_macroscopic(psl_grid* grid, double* host);
 int psl_set_populations(psl_grid* grid, const float* host);
 int psl_get_shifts(const psl_grid* grid, int* shifts27);
 int psl_set_shifts(psl_grid* grid, const int* shifts27);

@@ -571,16 +571,18 @@ static void updateLevel(Sim<T>& sim, int level) {  // flowAroundSphereMainSingle
   }
 }
 
-// fillEquilibrium.h:1-22 with the noisy-inflow start hook.
+// fillEquilibrium.h:1-22 with the noisy-inflow start hook; solid cells start at rest.
 template <typename T>
 static void fillEquilibrium(Sim<T>& sim, Grid<T>& g) {
   const Info& I = g.info;
   const CaseConfig& c = sim.cfg;
 #pragma omp parallel for schedule(static)
   for (long long cell = 0; cell < I.n; ++cell) {
-    const float ux = psl_noisy_velocity(c.uIn, c.noiseAmp, c.seed, (uint32_t)I.level, (uint32_t)cell, 0);
-    const float uy = psl_noisy_velocity(0.f, c.noiseAmp, c.seed, (uint32_t)I.level, (uint32_t)cell, 1);
-    const float uz = psl_noisy_velocity(0.f, c.noiseAmp, c.seed, (uint32_t)I.level, (uint32_t)cell, 2);
+    const int i = (int)(cell % I.nx), j = (int)((cell / I.nx) % I.ny), k = (int)(cell / ((long long)I.nx * I.ny));
+    const bool solid = cellKind(c, I, i, j, k) == Kind::Solid;
+    const float ux = solid ? 0.f : psl_noisy_velocity(c.uIn, c.noiseAmp, c.seed, (uint32_t)I.level, (uint32_t)cell, 0);
+    const float uy = solid ? 0.f : psl_noisy_velocity(0.f, c.noiseAmp, c.seed, (uint32_t)I.level, (uint32_t)cell, 1);
+    const float uz = solid ? 0.f : psl_noisy_velocity(0.f, c.noiseAmp, c.seed, (uint32_t)I.level, (uint32_t)cell, 2);
     T fe[27];
     feq(T(1), T(ux), T(uy), T(uz), fe);
     for (int q = 0; q < 27; ++q) g.f[(size_t)q * I.n + cell] = fe[q];

@@ -123,6 +123,10 @@ __cuda_callable__ void getInitialRhoUxUyUz(const int& iCell, const int& jCell, c
   getCellIndex(cell, iCell, jCell, kCell, Info);
   const uint32_t level = (uint32_t)Info.gridID;
   rho = 1.f;
+  if (Marker.bounceback) {  // solid cells start at rest
+    ux = uy = uz = 0.f;
+    return;
+  }
   ux = psl_noisy_velocity(g_case.uIn, g_case.noiseAmp, g_case.seed, level, (uint32_t)cell, 0);
   uy = psl_noisy_velocity(0.f, g_case.noiseAmp, g_case.seed, level, (uint32_t)cell, 1);
   uz = psl_noisy_velocity(0.f, g_case.noiseAmp, g_case.seed, level, (uint32_t)cell, 2);

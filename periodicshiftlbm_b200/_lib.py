@@ -12,8 +12,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("PSL_LIBRARY") or os.path.join(PKG, "libpsl_b200.so")
 
 PSL_OK = 0
-STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
-STORAGE_BYTES = {0: 4, 1: 2, 2: 2}
+STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3}
+STORAGE_BYTES = {0: 4, 1: 2, 2: 2, 3: 8}
 
 CELL_SKIP, CELL_FLUID, CELL_SOLID, CELL_GIVEN_U, CELL_GIVEN_RHO, CELL_GIVEN_NONE, CELL_GIVEN_BOTH, CELL_MIRROR = range(8)
 
@@ -78,6 +78,7 @@ _SIGNATURES = {
                                                            ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                                            ctypes.c_void_p, ctypes.c_void_p]),
     "psl_get_populations": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "psl_get_macroscopic": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_set_populations": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_get_shifts": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_set_shifts": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),

@@ -95,7 +95,7 @@ def make_sphere_grids(cfg: SphereConfig, storage: str = "f32") -> tuple:
     case = cfg.case()
     grids = []
     for info in cfg.infos():
-        g = GridStruct(info, storage=storage if info.gridID == 0 or storage == "f32" else storage)
+        g = GridStruct(info, storage=storage)
         setSphereCase(g, case)
         fillEquilibriumFromFunction(g, case)
         grids.append(g)

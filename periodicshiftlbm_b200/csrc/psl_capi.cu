@@ -128,6 +128,18 @@ static SphereCase sphere_hooks(const psl_sphere_case* sc) {
 
 static unsigned int blocks_for(size_t n, int threads) { return (unsigned int)((n + threads - 1) / threads); }
 
+// Calls fn with a value of the grid's storage type (StoreF32 / StoreF16 / StoreBF16 /
+// StoreF64) and returns what it returns.
+template <typename Fn>
+static auto with_storage(int storage, Fn&& fn) {
+  switch (storage) {
+    case kStoreF32: return fn(StoreF32{});
+    case kStoreF16: return fn(StoreF16{});
+    case kStoreBF16: return fn(StoreBF16{});
+    default: return fn(StoreF64{});
+  }
+}
+
 // Every psl_* definition below takes C linkage from its declaration in psl.h.
 
 const char* psl_last_error(void) { return g_last_error.c_str(); }
@@ -143,7 +155,7 @@ int psl_grid_create(const psl_info* info, int storage, psl_grid** out) {
   // which covers every grid except Ny = Nz = 1
   PSL_CHECK(!(ny == 1 && nz == 1), PSL_ERR_INVALID, "psl_grid_create: Ny = Nz = 1 grids are not supported");
   PSL_CHECK(n < (1LL << 31), PSL_ERR_INVALID, "psl_grid_create: more than 2^31-1 cells");
-  PSL_CHECK(storage >= 0 && storage <= 2, PSL_ERR_INVALID, "psl_grid_create: unknown storage");
+  PSL_CHECK(storage >= 0 && storage <= 3, PSL_ERR_INVALID, "psl_grid_create: unknown storage");
   const bool has_block = info->i_subgrid_end > info->i_subgrid_start;
   if (has_block) {
     PSL_CHECK(info->i_subgrid_start >= 0 && info->i_subgrid_end <= nx && info->j_subgrid_start >= 0 &&
@@ -276,11 +288,11 @@ template <typename Case>
 static int fill_eq(psl_grid* g, const Case& c) {
   DeviceGuard dg(g->device);
   const unsigned int nb = blocks_for(g->n, 256);
-  switch (g->storage) {
-    case kStoreF32: fill_equilibrium_kernel<StoreF32, Case><<<nb, 256, 0, g->stream>>>(view<StoreF32>(g), c, hook_info(g)); break;
-    case kStoreF16: fill_equilibrium_kernel<StoreF16, Case><<<nb, 256, 0, g->stream>>>(view<StoreF16>(g), c, hook_info(g)); break;
-    default: fill_equilibrium_kernel<StoreBF16, Case><<<nb, 256, 0, g->stream>>>(view<StoreBF16>(g), c, hook_info(g)); break;
-  }
+  with_storage(g->storage, [&](auto s) {
+    using S = decltype(s);
+    fill_equilibrium_kernel<S, Case><<<nb, 256, 0, g->stream>>>(view<S>(g), c, hook_info(g));
+    return 0;
+  });
   PSL_CUDA(cudaGetLastError());
   return PSL_OK;
 }
@@ -313,12 +325,13 @@ int psl_apply_streaming(psl_grid* g) {
   return PSL_OK;
 }
 
-static Relaxation relaxation(const psl_grid* g) {
-  Relaxation rx;
-  rx.tau = 3.f * g->info.nu + 0.5f;
+template <typename T>
+static RelaxationT<T> relaxation(const psl_grid* g) {
+  RelaxationT<T> rx;
+  rx.tau = T(3) * T(g->info.nu) + T(0.5);
   rx.tau2 = rx.tau * rx.tau;
-  rx.omega0 = 1.f / rx.tau;
-  rx.cs18 = 18.f * g->cs;
+  rx.omega0 = T(1) / rx.tau;
+  rx.cs18 = T(18) * T(g->cs);
   return rx;
 }
 
@@ -329,7 +342,7 @@ static void launch_step(psl_grid* g) {
   p.marker = g->marker;
   p.given = g->given;
   p.given_uniform = g->given_uniform;
-  p.rx = relaxation(g);
+  p.rx = relaxation<typename S::calc>(g);
   p.health = g->health;
   p.ri.base = static_cast<typename S::type*>(g->f);
   p.ri.n = g->n;
@@ -338,9 +351,13 @@ static void launch_step(psl_grid* g) {
     p.ri.lim[q] = g->n - g->shift[q];
   }
   const bool row_index = 27 * g->stride + g->n < (1ull << 32);
-  if (g->tiled && g->n % kTile == 0)
-    step_tiled_kernel<S><<<g->n / kTile, kTile, 0, g->stream>>>(p);
-  else if (row_index)
+  if constexpr (S::kind != kStoreF64) {
+    if (g->tiled && g->n % kTile == 0) {
+      step_tiled_kernel<S><<<g->n / kTile, kTile, 0, g->stream>>>(p);
+      return;
+    }
+  }
+  if (row_index)
     step_kernel<S, true><<<blocks_for(g->n, kStepThreads), kStepThreads, 0, g->stream>>>(p);
   else
     step_kernel<S, false><<<blocks_for(g->n, kStepThreads), kStepThreads, 0, g->stream>>>(p);
@@ -349,11 +366,10 @@ static void launch_step(psl_grid* g) {
 int psl_apply_local_cell_update(psl_grid* g) {
   PSL_CHECK(g, PSL_ERR_INVALID, "psl_apply_local_cell_update: null grid");
   DeviceGuard dg(g->device);
-  switch (g->storage) {
-    case kStoreF32: launch_step<StoreF32>(g); break;
-    case kStoreF16: launch_step<StoreF16>(g); break;
-    default: launch_step<StoreBF16>(g); break;
-  }
+  with_storage(g->storage, [&](auto s) {
+    launch_step<decltype(s)>(g);
+    return 0;
+  });
   PSL_CUDA(cudaGetLastError());
   return PSL_OK;
 }
@@ -371,33 +387,25 @@ static void launch_periodic(psl_grid* g, int axis) {
 static int periodic(psl_grid* g, int axis) {
   PSL_CHECK(g, PSL_ERR_INVALID, "psl_apply_bc_periodic: null grid");
   DeviceGuard dg(g->device);
-  switch (g->storage) {
-    case kStoreF32: launch_periodic<StoreF32>(g, axis); break;
-    case kStoreF16: launch_periodic<StoreF16>(g, axis); break;
-    default: launch_periodic<StoreBF16>(g, axis); break;
-  }
+  with_storage(g->storage, [&](auto s) {
+    launch_periodic<decltype(s)>(g, axis);
+    return 0;
+  });
   PSL_CUDA(cudaGetLastError());
   return PSL_OK;
 }
 int psl_apply_bc_periodic_x(psl_grid* g) { return periodic(g, 0); }
 int psl_apply_bc_periodic_y(psl_grid* g) { return periodic(g, 1); }
 
-int psl_apply_coarse_fine_grid_communication(psl_grid* c, psl_grid* f) {
-  PSL_CHECK(c && f, PSL_ERR_INVALID, "psl_apply_coarse_fine_grid_communication: null grid");
-  PSL_CHECK(c->storage == kStoreF32 && f->storage == kStoreF32, PSL_ERR_INVALID,
-            "psl_apply_coarse_fine_grid_communication: refinement needs FP32 storage");
+template <typename S>
+static int launch_coarse_fine(psl_grid* c, psl_grid* f) {
   const psl_info& C = c->info;
   const psl_info& F = f->info;
   const int a = C.i_subgrid_end - C.i_subgrid_start, b = C.j_subgrid_end - C.j_subgrid_start,
             cc = C.k_subgrid_end - C.k_subgrid_start;
-  PSL_CHECK(a >= 4 && b >= 4 && cc >= 4, PSL_ERR_INVALID, "coarse/fine: refinement block needs >= 4 cells per axis");
-  PSL_CHECK(F.cell_count_x == 2 * a && F.cell_count_y == 2 * b && F.cell_count_z == 2 * cc, PSL_ERR_INVALID,
-            "coarse/fine: fine grid is not twice the refinement block");
-  PSL_CHECK(c->device == f->device, PSL_ERR_INVALID, "coarse/fine: grids on different devices");
-  DeviceGuard dg(c->device);
-  CoarseFineParams p;
-  p.c = view<StoreF32>(c);
-  p.f = view<StoreF32>(f);
+  CoarseFineParams<S> p;
+  p.c = view<S>(c);
+  p.f = view<S>(f);
   p.cnx = C.cell_count_x;
   p.cny = C.cell_count_y;
   p.cnz = C.cell_count_z;
@@ -421,14 +429,31 @@ int psl_apply_coarse_fine_grid_communication(psl_grid* c, psl_grid* f) {
   p.error = c->health;
   int sms = 0, per_sm = 0;
   PSL_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-  PSL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_fine_kernel, kCoarseFineThreads, 0));
+  PSL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_fine_kernel<S>, kCoarseFineThreads, 0));
   PSL_CHECK(per_sm > 0, PSL_ERR_CUDA, "coarse/fine: kernel cannot be resident");
   const unsigned int want = blocks_for(std::max(p.n_ring, p.n_shell), kCoarseFineThreads);
   p.nblocks = std::min<unsigned int>((unsigned int)(sms * per_sm), std::max(1u, want));
   PSL_CUDA(cudaMemsetAsync(p.barrier, 0, sizeof(unsigned int), c->stream));
   void* args[] = {&p};
-  PSL_CUDA(cudaLaunchCooperativeKernel((const void*)coarse_fine_kernel, dim3(p.nblocks), dim3(kCoarseFineThreads), args, 0, c->stream));
+  PSL_CUDA(cudaLaunchCooperativeKernel((const void*)coarse_fine_kernel<S>, dim3(p.nblocks), dim3(kCoarseFineThreads),
+                                       args, 0, c->stream));
   return PSL_OK;
+}
+
+int psl_apply_coarse_fine_grid_communication(psl_grid* c, psl_grid* f) {
+  PSL_CHECK(c && f, PSL_ERR_INVALID, "psl_apply_coarse_fine_grid_communication: null grid");
+  PSL_CHECK(c->storage == f->storage, PSL_ERR_INVALID,
+            "psl_apply_coarse_fine_grid_communication: coarse and fine grids use different storage");
+  const psl_info& C = c->info;
+  const psl_info& F = f->info;
+  const int a = C.i_subgrid_end - C.i_subgrid_start, b = C.j_subgrid_end - C.j_subgrid_start,
+            cc = C.k_subgrid_end - C.k_subgrid_start;
+  PSL_CHECK(a >= 4 && b >= 4 && cc >= 4, PSL_ERR_INVALID, "coarse/fine: refinement block needs >= 4 cells per axis");
+  PSL_CHECK(F.cell_count_x == 2 * a && F.cell_count_y == 2 * b && F.cell_count_z == 2 * cc, PSL_ERR_INVALID,
+            "coarse/fine: fine grid is not twice the refinement block");
+  PSL_CHECK(c->device == f->device, PSL_ERR_INVALID, "coarse/fine: grids on different devices");
+  DeviceGuard dg(c->device);
+  return with_storage(c->storage, [&](auto s) { return launch_coarse_fine<decltype(s)>(c, f); });
 }
 
 int psl_update_grid(psl_grid** grids, int levels, int level) {
@@ -472,11 +497,10 @@ int psl_sphere_force(psl_grid* g, const psl_sphere_case* sc, double* force3) {
   if (i1 <= i0 || j1 <= j0 || k1 <= k0) return PSL_OK;
   const int si = i1 - i0, sj = j1 - j0, sk = k1 - k0;
   const int nb = (int)std::min<long long>(kForceBlocks, ((long long)si * sj * sk + 255) / 256);
-  switch (g->storage) {
-    case kStoreF32: launch_force<StoreF32>(g, i0, j0, k0, si, sj, sk, nb); break;
-    case kStoreF16: launch_force<StoreF16>(g, i0, j0, k0, si, sj, sk, nb); break;
-    default: launch_force<StoreBF16>(g, i0, j0, k0, si, sj, sk, nb); break;
-  }
+  with_storage(g->storage, [&](auto s) {
+    launch_force<decltype(s)>(g, i0, j0, k0, si, sj, sk, nb);
+    return 0;
+  });
   force_final_kernel<<<1, 32, 0, g->stream>>>(g->scratch, nb, g->scratch + kForceBlocks * 3);
   PSL_CUDA(cudaGetLastError());
   PSL_CUDA(cudaMemcpyAsync(force3, g->scratch + kForceBlocks * 3, 3 * sizeof(double), cudaMemcpyDeviceToHost, g->stream));
@@ -527,22 +551,33 @@ int psl_get_populations(psl_grid* g, float* host) {
   PSL_CHECK(g && host, PSL_ERR_INVALID, "psl_get_populations: null argument");
   DeviceGuard dg(g->device);
   PSL_CUDA(cudaStreamSynchronize(g->stream));
-  switch (g->storage) {
-    case kStoreF32: return gather<StoreF32>(g, host);
-    case kStoreF16: return gather<StoreF16>(g, host);
-    default: return gather<StoreBF16>(g, host);
-  }
+  return with_storage(g->storage, [&](auto s) { return gather<decltype(s)>(g, host); });
+}
+
+int psl_get_macroscopic(psl_grid* g, double* host) {
+  PSL_CHECK(g && host, PSL_ERR_INVALID, "psl_get_macroscopic: null argument");
+  DeviceGuard dg(g->device);
+  double* tmp = nullptr;
+  PSL_CUDA(cudaMalloc(&tmp, (size_t)g->n * 4 * sizeof(double)));
+  with_storage(g->storage, [&](auto s) {
+    using S = decltype(s);
+    macroscopic_kernel<S><<<blocks_for(g->n, 256), 256, 0, g->stream>>>(view<S>(g), tmp);
+    return 0;
+  });
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(host, tmp, (size_t)g->n * 4 * sizeof(double), cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return fail(PSL_ERR_CUDA, std::string("psl_get_macroscopic: ") + cudaGetErrorString(e));
+  return PSL_OK;
 }
 
 int psl_set_populations(psl_grid* g, const float* host) {
   PSL_CHECK(g && host, PSL_ERR_INVALID, "psl_set_populations: null argument");
   DeviceGuard dg(g->device);
   PSL_CUDA(cudaStreamSynchronize(g->stream));
-  switch (g->storage) {
-    case kStoreF32: return scatter<StoreF32>(g, host);
-    case kStoreF16: return scatter<StoreF16>(g, host);
-    default: return scatter<StoreBF16>(g, host);
-  }
+  return with_storage(g->storage, [&](auto s) { return scatter<decltype(s)>(g, host); });
 }
 
 int psl_get_shifts(const psl_grid* g, int* s) {

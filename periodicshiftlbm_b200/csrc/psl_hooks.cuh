@@ -115,12 +115,19 @@ struct SphereCase {
     uz = 0.f;
   }
   __device__ float getSmagorinskyConstant(int, int, int, const InfoStruct&) const { return smagorinsky; }
-  // feq(1, u_in + seeded noise): the noisy-inflow start of the sphere configurations
+  // feq(1, u_in + seeded noise): the noisy-inflow start of the sphere configurations.
+  // Solid cells start at rest (the variant the reference driver keeps commented out at
+  // flowAroundSphereMainSingle.cu:86-87), so the bounce-back interior of the sphere
+  // carries no momentum into the momentum-exchange drag sum.
   __device__ void getInitialRhoUxUyUz(int i, int j, int k, float& rho, float& ux, float& uy, float& uz,
-                                      const MarkerStruct&, const InfoStruct& I) const {
+                                      const MarkerStruct& M, const InfoStruct& I) const {
     const uint32_t cell = (uint32_t)(((long long)k * I.cellCountY + j) * I.cellCountX + i);
     const uint32_t level = (uint32_t)I.gridID;
     rho = 1.f;
+    if (M.bounceback) {
+      ux = uy = uz = 0.f;
+      return;
+    }
     ux = psl_noisy_velocity(uIn, noiseAmp, seed, level, cell, 0);
     uy = psl_noisy_velocity(0.f, noiseAmp, seed, level, cell, 1);
     uz = psl_noisy_velocity(0.f, noiseAmp, seed, level, cell, 2);
@@ -130,6 +137,7 @@ struct SphereCase {
 // ---- a uniform start state (fillEquilibrium with a constant hook) ----
 struct UniformCase {
   float rho0, ux0, uy0, uz0;
+  __device__ void getMarkers(int, int, int, MarkerStruct& M, const InfoStruct&) const { M.fluid = 1; }
   __device__ void getInitialRhoUxUyUz(int, int, int, float& rho, float& ux, float& uy, float& uz, const MarkerStruct&,
                                       const InfoStruct&) const {
     rho = rho0;

@@ -56,15 +56,16 @@ struct StepParams {
   const uint8_t* marker;
   const float4* given;   // per-cell (rho, ux, uy, uz) for boundary cells, or null
   float4 given_uniform;  // used when `given` is null
-  Relaxation rx;
+  RelaxationT<typename S::calc> rx;
   unsigned int* health;  // bit 0 set when a collided cell's density is not finite/positive
 };
 
 // The boundary branch runs for ~2% of cells; keeping it out of line keeps the hot path's
 // instruction footprint small.  (applyLocalCellUpdate.h:41-67)
-static __device__ __noinline__ void apply_boundary(uint8_t m, float (&f)[27], float4 given) {
+template <typename T>
+static __device__ __noinline__ void apply_boundary(uint8_t m, T (&f)[27], float4 given) {
   const int kind = marker_kind(m), normal = marker_normal(m);
-  float rho = given.x, ux = given.y, uy = given.z, uz = given.w;
+  T rho = given.x, ux = given.y, uy = given.z, uz = given.w;
   if (kind == kMirror) {
     bc::mirror(normal, f);
     return;
@@ -76,14 +77,14 @@ static __device__ __noinline__ void apply_boundary(uint8_t m, float (&f)[27], fl
 }
 
 template <typename S, int Q = 0>
-__device__ __forceinline__ void load_cell(const GridView<S>& g, uint32_t cell, float (&f)[27]) {
+__device__ __forceinline__ void load_cell(const GridView<S>& g, uint32_t cell, typename S::calc (&f)[27]) {
   if constexpr (Q < 27) {
     f[Q] = S::template load<Q>(g.fq[Q] + shifted(cell, g.shift[Q], g.n));
     load_cell<S, Q + 1>(g, cell, f);
   }
 }
 template <typename S, int Q = 0>
-__device__ __forceinline__ void store_cell(const GridView<S>& g, uint32_t cell, const float (&f)[27]) {
+__device__ __forceinline__ void store_cell(const GridView<S>& g, uint32_t cell, const typename S::calc (&f)[27]) {
   if constexpr (Q < 27) {
     S::template store<Q>(g.fq[Q] + shifted(cell, g.shift[Q], g.n), f[Q]);
     store_cell<S, Q + 1>(g, cell, f);
@@ -91,7 +92,7 @@ __device__ __forceinline__ void store_cell(const GridView<S>& g, uint32_t cell, 
 }
 
 template <typename S, int Q = 0>
-__device__ __forceinline__ void load_cell_ri(const RowIndex<S>& r, uint32_t cell, float (&f)[27]) {
+__device__ __forceinline__ void load_cell_ri(const RowIndex<S>& r, uint32_t cell, typename S::calc (&f)[27]) {
   if constexpr (Q < 27) {
     uint32_t i = cell + r.off[Q];
     if (cell >= r.lim[Q]) i -= r.n;
@@ -100,7 +101,7 @@ __device__ __forceinline__ void load_cell_ri(const RowIndex<S>& r, uint32_t cell
   }
 }
 template <typename S, int Q = 0>
-__device__ __forceinline__ void store_cell_ri(const RowIndex<S>& r, uint32_t cell, const float (&f)[27]) {
+__device__ __forceinline__ void store_cell_ri(const RowIndex<S>& r, uint32_t cell, const typename S::calc (&f)[27]) {
   if constexpr (Q < 27) {
     uint32_t i = cell + r.off[Q];
     if (cell >= r.lim[Q]) i -= r.n;
@@ -116,13 +117,14 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constan
   const uint8_t m = p.marker[cell];
   const int kind = marker_kind(m);
   if (kind == kSkip) return;
-  float f[27];
+  using T = typename S::calc;
+  T f[27];
   if constexpr (kRowIndex) load_cell_ri<S>(p.ri, cell, f);
   else load_cell<S>(p.g, cell, f);
   if (kind == kSolid) {
 #pragma unroll
     for (int q = 1; q < 27; q += 2) {
-      const float t = f[q];
+      const T t = f[q];
       f[q] = f[q + 1];
       f[q + 1] = t;
     }
@@ -130,8 +132,8 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constan
     if (kind != kFluid) apply_boundary(m, f, p.given ? p.given[cell] : p.given_uniform);
     collide<false>(f, p.rx);
     if (p.health) {
-      const float r = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6];
-      if (!(r > 0.f && r < 1.0e30f)) atomicOr(p.health, 1u);
+      const T r = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6];
+      if (!(r > T(0) && r < T(1.0e30))) atomicOr(p.health, 1u);
     }
   }
   if constexpr (kRowIndex) store_cell_ri<S>(p.ri, cell, f);
@@ -167,12 +169,13 @@ __global__ void fill_markers_kernel(Case c, InfoStruct I, uint32_t n, uint8_t* m
 }
 
 // second-order equilibrium (include/cellFunctions.h:60-121)
-__device__ __forceinline__ void equilibrium(float rho, float ux, float uy, float uz, float (&fe)[27]) {
-  const float u2 = ux * ux + uy * uy + uz * uz;
+template <typename T>
+__device__ __forceinline__ void equilibrium(T rho, T ux, T uy, T uz, T (&fe)[27]) {
+  const T u2 = ux * ux + uy * uy + uz * uz;
 #pragma unroll
   for (int q = 0; q < 27; ++q) {
-    const float cu = (float)cx(q) * ux + (float)cy(q) * uy + (float)cz(q) * uz;
-    fe[q] = rho * lattice_weight(q) * (1.f + 3.f * cu + 4.5f * cu * cu - 1.5f * u2);
+    const T cu = (T)cx(q) * ux + (T)cy(q) * uy + (T)cz(q) * uz;
+    fe[q] = rho * weight_t<T>(q) * (T(1) + T(3) * cu + T(4.5) * cu * cu - T(1.5) * u2);
   }
 }
 
@@ -183,10 +186,12 @@ __global__ void fill_equilibrium_kernel(GridView<S> g, Case c, InfoStruct I) {
   int i, j, k;
   cell_ijk(cell, I, i, j, k);
   MarkerStruct M;
+  c.getMarkers(i, j, k, M, I);  // the start hook sees the cell's markers (fillEquilibrium.h:15-16)
   float rho = 1.f, ux = 0.f, uy = 0.f, uz = 0.f;
   c.getInitialRhoUxUyUz(i, j, k, rho, ux, uy, uz, M, I);
-  float fe[27];
-  equilibrium(rho, ux, uy, uz, fe);
+  using T = typename S::calc;
+  T fe[27];
+  equilibrium<T>(rho, ux, uy, uz, fe);
   store_cell<S>(g, cell, fe);
 }
 
@@ -236,9 +241,10 @@ __global__ void periodic_kernel(GridView<S> g, int nx, int ny, int nz) {
 //   since every launch computes the same value for a given fine cell, the union is the
 //   same final state.
 // ------------------------------------------------------------------------------------------
+template <typename S>
 struct CoarseFineParams {
-  GridView<StoreF32> c;
-  GridView<StoreF32> f;
+  GridView<S> c;
+  GridView<S> f;
   int cnx, cny, cnz;
   int iS, jS, kS, iE, jE, kE;
   int fnx, fny, fnz;
@@ -281,9 +287,13 @@ __device__ __forceinline__ void grid_barrier(unsigned int* counter, unsigned int
 // Coarse reads after the grid barrier use ordinary (L1-cached) loads: no SM read a coarse
 // line before the barrier in this launch, and L1 starts empty for every launch, so no
 // stale copy of a restricted ring cell can be hit.
-__device__ __forceinline__ void load_cell_plain(const GridView<StoreF32>& g, uint32_t cell, float (&f)[27]) {
-#pragma unroll
-  for (int q = 0; q < 27; ++q) f[q] = g.fq[q][shifted(cell, g.shift[q], g.n)];
+template <typename S>
+__device__ __forceinline__ typename S::calc load_pop(const GridView<S>& g, int q, uint32_t cell) {
+  return S::load_q(g.fq[q] + shifted(cell, g.shift[q], g.n), q);
+}
+template <typename S>
+__device__ __forceinline__ void store_pop(const GridView<S>& g, int q, uint32_t cell, typename S::calc v) {
+  S::store_q(g.fq[q] + shifted(cell, g.shift[q], g.n), v, q);
 }
 
 // Work items are dealt out in warp-sized chunks, consecutive chunks to consecutive blocks,
@@ -295,7 +305,9 @@ __device__ __forceinline__ void load_cell_plain(const GridView<StoreF32>& g, uin
 
 constexpr int kCoarseFineThreads = 128;
 
-static __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const __grid_constant__ CoarseFineParams p) {
+template <typename S>
+__global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const __grid_constant__ CoarseFineParams<S> p) {
+  using T = typename S::calc;
   // ---------------- phase 1: restriction ----------------
   {
     const int a = p.iE - p.iS - 2, b = p.jE - p.jS - 2, c = p.kE - p.kS - 2;  // ring box extents
@@ -321,9 +333,9 @@ static __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(
       }
       const int i = p.iS + 1 + ri, j = p.jS + 1 + rj, k = p.kS + 1 + rk;
       const int fi = (i - p.iS) * 2, fj = (j - p.jS) * 2, fk = (k - p.kS) * 2;
-      float f[27];
+      T f[27];
 #pragma unroll
-      for (int q = 0; q < 27; ++q) f[q] = 0.f;
+      for (int q = 0; q < 27; ++q) f[q] = T(0);
 #pragma unroll
       for (int dk = 0; dk <= 1; ++dk)
 #pragma unroll
@@ -332,14 +344,14 @@ static __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(
           for (int di = 0; di <= 1; ++di) {
             const uint32_t fc = ((uint32_t)(fk + dk) * p.fny + (fj + dj)) * p.fnx + (fi + di);
 #pragma unroll
-            for (int q = 0; q < 27; ++q) f[q] = __fadd_rn(f[q], p.f.fq[q][shifted(fc, p.f.shift[q], p.f.n)]);
+            for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], load_pop(p.f, q, fc));
           }
 #pragma unroll
-      for (int q = 0; q < 27; ++q) f[q] = f[q] * 0.125f;
+      for (int q = 0; q < 27; ++q) f[q] = f[q] * T(0.125);
       rescale(f, false);
       const uint32_t cc = ((uint32_t)k * p.cny + j) * p.cnx + i;
 #pragma unroll
-      for (int q = 0; q < 27; ++q) p.c.fq[q][shifted(cc, p.c.shift[q], p.c.n)] = f[q];
+      for (int q = 0; q < 27; ++q) store_pop(p.c, q, cc, f[q]);
     }
   }
   grid_barrier(p.barrier, p.nblocks, p.error);
@@ -381,31 +393,33 @@ static __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(
     }
     if (!mask) continue;
     const int ic = i / 2 + p.iS, jc = j / 2 + p.jS, kc = k / 2 + p.kS;
-    const float d[3] = {(i & 1) ? 0.25f : -0.25f, (j & 1) ? 0.25f : -0.25f, (k & 1) ? 0.25f : -0.25f};
-    float f[27];
-    load_cell_plain(p.c, ((uint32_t)kc * p.cny + jc) * p.cnx + ic, f);
+    const T d[3] = {T((i & 1) ? 0.25f : -0.25f), T((j & 1) ? 0.25f : -0.25f), T((k & 1) ? 0.25f : -0.25f)};
+    T f[27];
+    const uint32_t pc = ((uint32_t)kc * p.cny + jc) * p.cnx + ic;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) f[q] = load_pop(p.c, q, pc);
     const int cidx[3] = {ic, jc, kc};
     const int cdim[3] = {p.cnx, p.cny, p.cnz};
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
       int plus = cidx[ax] + 1, minus = cidx[ax] - 1;
-      float inv = 0.5f;
-      if (plus >= cdim[ax]) { plus = cidx[ax]; inv = 1.f; }
-      if (minus < 0) { minus = 0; inv = 1.f; }
+      T inv = T(0.5);
+      if (plus >= cdim[ax]) { plus = cidx[ax]; inv = T(1); }
+      if (minus < 0) { minus = 0; inv = T(1); }
 #pragma unroll
       for (int side = 0; side < 2; ++side) {
         int nb[3] = {ic, jc, kc};
         nb[ax] = side == 0 ? plus : minus;
-        const float w = (side == 0 ? inv : -inv) * d[ax];  // exact: powers of two
+        const T w = (side == 0 ? inv : -inv) * d[ax];  // exact: powers of two
         const uint32_t nc = ((uint32_t)nb[2] * p.cny + nb[1]) * p.cnx + nb[0];
 #pragma unroll
-        for (int q = 0; q < 27; ++q) f[q] = __fadd_rn(f[q], p.c.fq[q][shifted(nc, p.c.shift[q], p.c.n)] * w);
+        for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], load_pop(p.c, q, nc) * w);
       }
     }
     rescale(f, true);
 #pragma unroll
     for (int q = 0; q < 27; ++q)
-      if (mask & (1u << q)) p.f.fq[q][shifted(fcell, p.f.shift[q], p.f.n)] = f[q];
+      if (mask & (1u << q)) store_pop(p.f, q, fcell, f[q]);
   }
 }
 
@@ -476,6 +490,28 @@ __global__ void scatter_logical_kernel(GridView<S> g, int q, const float* in) {
   const uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x;
   if (cell >= g.n) return;
   S::store_q(g.fq[q] + shifted(cell, g.shift[q], g.n), in[cell], q);
+}
+
+// Density and velocity of every cell in FP64 (getRhoUxUyUz, cellFunctions.h:135-155),
+// written as four logical-order planes.
+template <typename S>
+__global__ void macroscopic_kernel(GridView<S> g, double* out) {
+  const uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= g.n) return;
+  double rho = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+  for (int q = 0; q < 27; ++q) {
+    const double v = (double)S::load_q(g.fq[q] + shifted(cell, g.shift[q], g.n), q);
+    rho += v;
+    jx += cx(q) * v;
+    jy += cy(q) * v;
+    jz += cz(q) * v;
+  }
+  const size_t n = g.n;
+  out[cell] = rho;
+  out[n + cell] = jx / rho;
+  out[2 * n + cell] = jy / rho;
+  out[3 * n + cell] = jz / rho;
 }
 
 // ------------------------------------------------------------------------------------------

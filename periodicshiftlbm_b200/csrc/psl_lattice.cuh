@@ -31,6 +31,12 @@ PSL_HDI constexpr float lattice_weight(int q) {
   return q == 0 ? 8.f / 27.f : (q <= 6 ? 2.f / 27.f : (q <= 18 ? 1.f / 54.f : 1.f / 216.f));
 }
 
+// The same weights in the arithmetic type T (the FP64 form rounds 8/27 etc. in double).
+template <typename T>
+PSL_HDI constexpr T weight_t(int q) {
+  return q == 0 ? T(8) / T(27) : (q <= 6 ? T(2) / T(27) : (q <= 18 ? T(1) / T(54) : T(1) / T(216)));
+}
+
 PSL_HDI constexpr int opposite(int q) { return q == 0 ? 0 : ((q & 1) ? q + 1 : q - 1); }
 
 // Population index of velocity (x, y, z) in {-1,0,1}^3 ("slot" of the central-moment

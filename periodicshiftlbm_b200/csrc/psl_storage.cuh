@@ -1,11 +1,13 @@
-// Population storage formats.  All arithmetic is FP32; only the bytes in HBM differ.
+// Population storage formats.  `type` is the element in HBM, `calc` the arithmetic type
+// of the update (FP32 for every production form; FP64 only for the FP64 oracle runs).
 //
 //   F32            f_q stored as is                       (216 B moved per cell update)
 //   F16 / BF16     f_q - w_q stored in 16 bits            (108 B per cell update)
+//   F64            f_q stored as is, FP64 arithmetic      (432 B; oracle runs only)
 //
 // Storing the deviation from the lattice weight keeps the stored values small (|f - w|
 // is O(u) relative to w), so the 16-bit formats spend their mantissa on the part that
-// changes.  The north_star precision form.
+// changes.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -14,10 +16,11 @@
 
 namespace psl {
 
-enum StorageKind : int { kStoreF32 = 0, kStoreF16 = 1, kStoreBF16 = 2 };
+enum StorageKind : int { kStoreF32 = 0, kStoreF16 = 1, kStoreBF16 = 2, kStoreF64 = 3 };
 
 struct StoreF32 {
   using type = float;
+  using calc = float;
   static constexpr int kind = kStoreF32;
   template <int Q>
   __device__ __forceinline__ static float load(const float* p) { return *p; }
@@ -35,6 +38,7 @@ struct StoreF32 {
 
 struct StoreF16 {
   using type = __half;
+  using calc = float;
   static constexpr int kind = kStoreF16;
   template <int Q>
   __device__ __forceinline__ static float load(const __half* p) { return __half2float(*p) + lattice_weight(Q); }
@@ -52,6 +56,7 @@ struct StoreF16 {
 
 struct StoreBF16 {
   using type = __nv_bfloat16;
+  using calc = float;
   static constexpr int kind = kStoreBF16;
   template <int Q>
   __device__ __forceinline__ static float load(const __nv_bfloat16* p) { return __bfloat162float(*p) + lattice_weight(Q); }
@@ -73,6 +78,22 @@ struct StoreBF16 {
   }
 };
 
-inline size_t storage_bytes(int kind) { return kind == kStoreF32 ? 4 : 2; }
+struct StoreF64 {
+  using type = double;
+  using calc = double;
+  static constexpr int kind = kStoreF64;
+  template <int Q>
+  __device__ __forceinline__ static double load(const double* p) { return *p; }
+  template <int Q>
+  __device__ __forceinline__ static void store(double* p, double v) { *p = v; }
+  __device__ __forceinline__ static double load_q(const double* p, int) { return *p; }
+  __device__ __forceinline__ static void store_q(double* p, double v, int) { *p = v; }
+  template <int Q>
+  __device__ __forceinline__ static double load_once(const double* p) { return __ldg(p); }
+  template <int Q>
+  __device__ __forceinline__ static void store_once(double* p, double v) { __stcs(p, v); }
+};
+
+inline size_t storage_bytes(int kind) { return kind == kStoreF32 ? 4 : kind == kStoreF64 ? 8 : 2; }
 
 }  // namespace psl

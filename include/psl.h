@@ -143,6 +143,43 @@ int psl_momentum_exchange_force_noalloc(const float* populations, long long row_
                                         long long cell_count, const uint8_t* markers, int nx, int ny, int nz,
                                         const int* box_lo3, const int* box_hi3, double* force3, void* cuda_stream);
 
+/* ---- batched form ----
+ * Many independent single-level grids (e.g. sphere cases of different sizes and Reynolds
+ * numbers) advanced together: each step is ONE persistent kernel over the tiles of all
+ * member grids plus a one-thread kernel that advances a device step counter; the grids'
+ * periodic shifts are derived from that counter on the device, so the step is captured
+ * once in a CUDA graph and replayed.  No reference counterpart: the reference advances
+ * one grid hierarchy per process.  Members must share device and storage, have no
+ * refinement block and stay alive while the batch exists (psl_grid_destroy refuses a
+ * member grid).  A member grid's own calls (psl_sphere_force, psl_get_populations, ...)
+ * stay valid between batch runs: psl_batch_run brings the grid's shifts up to date and
+ * orders the grid's stream after the batch's work.  The batch reads each grid's viscosity,
+ * Smagorinsky constant and given values when it is created (or retuned); a member grid
+ * streamed on its own fails the next psl_batch_run. */
+typedef struct psl_batch psl_batch;
+typedef struct psl_batch_tuning {
+  int threads;       /* threads per CTA: a multiple of 32, at most 256 */
+  int tile_cells;    /* consecutive cells per tile: a multiple of threads */
+  int blocks_per_sm; /* resident CTAs per SM in the persistent grid */
+  float ms_per_step; /* time per step measured by psl_batch_autotune (0 if not tuned) */
+} psl_batch_tuning;
+int psl_batch_create(psl_grid* const* grids, int count, psl_batch** out);
+int psl_batch_destroy(psl_batch* batch);
+/* Advance every member grid by `steps` steps (graph replays on the batch's stream; not
+ * synchronised). */
+int psl_batch_run(psl_batch* batch, int steps);
+int psl_batch_synchronize(psl_batch* batch);
+/* The batch's own CUDA stream (created non-blocking), for timing with events. */
+int psl_batch_get_stream(const psl_batch* batch, void** stream);
+int psl_batch_get_tuning(const psl_batch* batch, psl_batch_tuning* tuning);
+int psl_batch_set_tuning(psl_batch* batch, const psl_batch_tuning* tuning);
+/* Project-written autotuner: times every candidate launch shape (threads 64/128/256 x
+ * tile 1-16 x threads x {max, max/2} resident CTAs per SM) over `trial_steps` steps on the
+ * batch itself, adopts the fastest and reports it in *chosen.  The populations and the
+ * step counter are saved first and restored afterwards, so tuning does not advance the
+ * simulation. */
+int psl_batch_autotune(psl_batch* batch, int trial_steps, psl_batch_tuning* chosen);
+
 /* ---- data movement ---- */
 /* Populations in logical order: host[q * N + cell] = f_q of `cell` (FP32 for every storage). */
 int psl_get_populations(psl_grid* grid, float* host);

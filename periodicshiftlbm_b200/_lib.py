@@ -44,6 +44,15 @@ class PslSphereCase(ctypes.Structure):
     ]
 
 
+class PslBatchTuning(ctypes.Structure):
+    _fields_ = [
+        ("threads", ctypes.c_int),
+        ("tile_cells", ctypes.c_int),
+        ("blocks_per_sm", ctypes.c_int),
+        ("ms_per_step", ctypes.c_float),
+    ]
+
+
 class PslError(RuntimeError):
     pass
 
@@ -79,6 +88,14 @@ _SIGNATURES = {
                                                            ctypes.c_void_p, ctypes.c_void_p]),
     "psl_get_populations": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_get_macroscopic": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "psl_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "psl_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "psl_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "psl_batch_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "psl_batch_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "psl_batch_get_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PslBatchTuning)]),
+    "psl_batch_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PslBatchTuning)]),
+    "psl_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(PslBatchTuning)]),
     "psl_set_populations": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_get_shifts": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_set_shifts": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),

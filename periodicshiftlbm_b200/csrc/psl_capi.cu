@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "psl.h"
+#include "psl_internal.h"
 #include "psl_kernels.cuh"
 #include "psl_step_tiled.cuh"
 
@@ -39,41 +40,6 @@ __attribute__((visibility("hidden"))) void psl_detail_set_last_error(const std::
   do {                             \
     if (!(cond)) return fail(code, msg); \
   } while (0)
-
-// Make the grid's device current for the duration of a call, restoring the caller's.
-struct DeviceGuard {
-  int prev = -1;
-  bool ok = true;
-  explicit DeviceGuard(int dev) {
-    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-    if (prev != dev) ok = (cudaSetDevice(dev) == cudaSuccess);
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-  }
-};
-
-// ------------------------------------------------------------------------------------------
-// grid
-// ------------------------------------------------------------------------------------------
-struct psl_grid {
-  psl_info info;
-  uint32_t n = 0;
-  int storage = 0;
-  size_t stride = 0;  // elements per population row, multiple of 64 (128-byte rows)
-  void* f = nullptr;
-  uint8_t* marker = nullptr;
-  float4* given = nullptr;
-  float4 given_uniform = make_float4(1.f, 0.f, 0.f, 0.f);
-  float cs = 0.f;
-  uint32_t shift[27] = {};
-  cudaStream_t stream = 0;
-  unsigned int* health = nullptr;   // [0] health bits, [1] barrier counter
-  double* scratch = nullptr;        // force partials (kForceBlocks x 3) + result (3)
-  int device = 0;
-  bool tiled = false;               // bulk-copy tiled update kernel (N % 128 == 0)
-};
 
 static constexpr int kForceBlocks = 512;
 
@@ -195,6 +161,7 @@ int psl_grid_create(const psl_info* info, int storage, psl_grid** out) {
 
 int psl_grid_destroy(psl_grid* g) {
   if (!g) return PSL_OK;
+  PSL_CHECK(g->batched == 0, PSL_ERR_INVALID, "psl_grid_destroy: the grid belongs to a live batch");
   DeviceGuard dg(g->device);
   if (g->f) cudaFree(g->f);
   if (g->marker) cudaFree(g->marker);

@@ -1,0 +1,50 @@
+// Library-internal declarations shared by the C ABI translation units (psl_capi.cu,
+// psl_batch.cu, psl_noalloc.cu): the grid object behind the opaque psl_grid handle and
+// small host helpers.  Not part of the public interface.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "psl.h"
+
+// Sets psl_last_error() for the calling thread (defined in psl_capi.cu).
+__attribute__((visibility("hidden"))) void psl_detail_set_last_error(const std::string& msg);
+
+// Make the grid's device current for the duration of a call, restoring the caller's.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) ok = (cudaSetDevice(dev) == cudaSuccess);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// ------------------------------------------------------------------------------------------
+// grid
+// ------------------------------------------------------------------------------------------
+struct psl_grid {
+  psl_info info;
+  uint32_t n = 0;
+  int storage = 0;
+  size_t stride = 0;  // elements per population row, multiple of 64 (128-byte rows)
+  void* f = nullptr;
+  uint8_t* marker = nullptr;
+  float4* given = nullptr;
+  float4 given_uniform = make_float4(1.f, 0.f, 0.f, 0.f);
+  float cs = 0.f;
+  uint32_t shift[27] = {};
+  cudaStream_t stream = 0;
+  unsigned int* health = nullptr;   // [0] health bits, [1] barrier counter
+  double* scratch = nullptr;        // force partials (kForceBlocks x 3) + result (3)
+  int device = 0;
+  bool tiled = false;               // bulk-copy tiled update kernel (N % 128 == 0)
+  int batched = 0;                  // member of this many live batches (psl_batch.cu)
+};
+

@@ -110,6 +110,28 @@ __device__ __forceinline__ void store_cell_ri(const RowIndex<S>& r, uint32_t cel
   }
 }
 
+// The per-cell body (applyLocalCellUpdate.h:21-72): bounce-back for solid cells; for the
+// others the boundary condition of the marker, the collision and a density health check.
+template <typename T>
+__device__ __forceinline__ void local_cell_update(int kind, uint8_t m, T (&f)[27], const float4* given, float4 given_uniform,
+                                                  uint32_t cell, const RelaxationT<T>& rx, unsigned int* health) {
+  if (kind == kSolid) {
+#pragma unroll
+    for (int q = 1; q < 27; q += 2) {
+      const T t = f[q];
+      f[q] = f[q + 1];
+      f[q + 1] = t;
+    }
+  } else {
+    if (kind != kFluid) apply_boundary(m, f, given ? given[cell] : given_uniform);
+    collide<false>(f, rx);
+    if (health) {
+      const T r = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6];
+      if (!(r > T(0) && r < T(1.0e30))) atomicOr(health, 1u);
+    }
+  }
+}
+
 template <typename S, bool kRowIndex>
 __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constant__ StepParams<S> p) {
   const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
@@ -117,6 +139,8 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constan
   const uint8_t m = p.marker[cell];
   const int kind = marker_kind(m);
   if (kind == kSkip) return;
+  // (the body of local_cell_update, written out: nvcc allocates 56 registers for this
+  // form against 64 through the helper)
   using T = typename S::calc;
   T f[27];
   if constexpr (kRowIndex) load_cell_ri<S>(p.ri, cell, f);

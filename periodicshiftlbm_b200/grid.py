@@ -126,7 +126,7 @@ class GridStruct:
 
     def close(self):
         if self._h and self._h.value:
-            _lib.lib().psl_grid_destroy(self._h)
+            call("psl_grid_destroy", self._h)  # refuses (raises) while the grid is in a batch
             self._h = ctypes.c_void_p()
 
     def __del__(self):

@@ -143,6 +143,34 @@ int psl_momentum_exchange_force_noalloc(const float* populations, long long row_
                                         long long cell_count, const uint8_t* markers, int nx, int ny, int nz,
                                         const int* box_lo3, const int* box_hi3, double* force3, void* cuda_stream);
 
+/* ---- learned subgrid closure ----
+ * A per-cell MLP (10 features -> 32 -> 32 -> 1, ReLU, softplus output) that replaces the
+ * Smagorinsky rate of getOmegaLES (cellFunctions.h:157-198): omega = 1/(3 (nu + nu_t) + 1/2).
+ * No reference counterpart.  Features of a cell, from its post-streaming populations after
+ * the boundary condition: Pi = (C - rho/3 I)/rho with C the second-order central moments,
+ * x = (Pi_xx, Pi_yy, Pi_zz, Pi_xy, Pi_xz, Pi_yz, tr Pi, |Pi|, det Pi / |Pi|^2, width); the
+ * network sees (x - in_shift) * in_scale.  Weights are rounded to FP16 on the device and
+ * evaluated on the tensor cores with FP32 accumulation. */
+typedef struct psl_sgs_mlp {
+  float w1[32][10];  /* layer 1: h1 = relu(w1 x' + b1) */
+  float b1[32];
+  float w2[32][32];  /* layer 2: h2 = relu(w2 h1 + b2) */
+  float b2[32];
+  float w3[32];      /* output: nu_t = out_scale * softplus(w3 . h2 + b3) */
+  float b3;
+  float in_shift[10];
+  float in_scale[10];
+  float out_scale;
+} psl_sgs_mlp;
+/* Use the closure in psl_apply_local_cell_update of `grid` (NULL: back to Smagorinsky).
+ * `filter_width` is the width feature of this grid (its cell size over the coarsest
+ * grid's).  Cells fall back to Smagorinsky if the closure's tensor-core step times out
+ * (health bit 2). */
+int psl_set_sgs_mlp(psl_grid* grid, const psl_sgs_mlp* mlp, float filter_width);
+/* The closure alone on host features (count x 10 raw features) -> nu_t (count floats),
+ * through the same tensor-core device code (parity tests). */
+int psl_sgs_mlp_infer(const psl_sgs_mlp* mlp, const float* features, int count, float* nu_t);
+
 /* ---- batched form ----
  * Many independent single-level grids (e.g. sphere cases of different sizes and Reynolds
  * numbers) advanced together: each step is ONE persistent kernel over the tiles of all
@@ -193,7 +221,7 @@ int psl_get_shifts(const psl_grid* grid, int* shifts27);
 int psl_set_shifts(psl_grid* grid, const int* shifts27);
 int psl_synchronize(psl_grid* grid);
 /* Health word of the update kernels (bit 0: non-finite density seen; bit 1: a grid
- * barrier timed out); read and clear. */
+ * barrier timed out; bit 2: a wait of the learned closure timed out); read and clear. */
 int psl_check_health(psl_grid* grid, unsigned int* flags);
 
 /* ---- single-cell entry points (unit parity of the device functions) ----

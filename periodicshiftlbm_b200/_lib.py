@@ -53,6 +53,20 @@ class PslBatchTuning(ctypes.Structure):
     ]
 
 
+class PslSgsMlp(ctypes.Structure):
+    _fields_ = [
+        ("w1", (ctypes.c_float * 10) * 32),
+        ("b1", ctypes.c_float * 32),
+        ("w2", (ctypes.c_float * 32) * 32),
+        ("b2", ctypes.c_float * 32),
+        ("w3", ctypes.c_float * 32),
+        ("b3", ctypes.c_float),
+        ("in_shift", ctypes.c_float * 10),
+        ("in_scale", ctypes.c_float * 10),
+        ("out_scale", ctypes.c_float),
+    ]
+
+
 class PslError(RuntimeError):
     pass
 
@@ -88,6 +102,8 @@ _SIGNATURES = {
                                                            ctypes.c_void_p, ctypes.c_void_p]),
     "psl_get_populations": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_get_macroscopic": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "psl_set_sgs_mlp": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PslSgsMlp), ctypes.c_float]),
+    "psl_sgs_mlp_infer": (ctypes.c_int, [ctypes.POINTER(PslSgsMlp), ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "psl_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "psl_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "psl_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

@@ -25,7 +25,8 @@ NVCC_FLAGS = [
     "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
     "-shared", "-Xcompiler", "-fPIC",
 ]
-SOURCES = [os.path.join(CSRC, "psl_capi.cu"), os.path.join(CSRC, "psl_noalloc.cu"), os.path.join(CSRC, "psl_batch.cu")]
+SOURCES = [os.path.join(CSRC, "psl_capi.cu"), os.path.join(CSRC, "psl_noalloc.cu"), os.path.join(CSRC, "psl_batch.cu"),
+           os.path.join(CSRC, "psl_learned.cu")]
 
 
 def _nvcc() -> str:

@@ -168,6 +168,7 @@ int psl_grid_destroy(psl_grid* g) {
   if (g->given) cudaFree(g->given);
   if (g->health) cudaFree(g->health);
   if (g->scratch) cudaFree(g->scratch);
+  if (g->mlp) cudaFree(g->mlp);
   delete g;
   return PSL_OK;
 }
@@ -333,6 +334,7 @@ static void launch_step(psl_grid* g) {
 int psl_apply_local_cell_update(psl_grid* g) {
   PSL_CHECK(g, PSL_ERR_INVALID, "psl_apply_local_cell_update: null grid");
   DeviceGuard dg(g->device);
+  if (g->mlp) return psl_detail_launch_learned(g);
   with_storage(g->storage, [&](auto s) {
     launch_step<decltype(s)>(g);
     return 0;

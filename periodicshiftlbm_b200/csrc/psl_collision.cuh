@@ -216,6 +216,53 @@ struct RelaxationT {
 };
 using Relaxation = RelaxationT<float>;
 
+// Relaxation of the second-order cumulants at shear rate w (bulk at 1, higher cumulants
+// to 0; Geier 2015 eqs 55-65, include/applyCollision.h:119-200) and the inverse transform.
+template <typename T>
+__device__ __forceinline__ void relax_rebuild(T (&f)[27], const T (&K)[3][3][3], T rho, T ux, T uy, T uz, T inv_rho,
+                                              T w) {
+  const T k000 = K[0][0][0], k100 = K[1][0][0], k010 = K[0][1][0], k001 = K[0][0][1];
+  const T c200 = K[2][0][0], c020 = K[0][2][0], c002 = K[0][0][2];
+  const T c011 = K[0][1][1], c101 = K[1][0][1], c110 = K[1][1][0];
+  const T hw = T(0.5) * w * inv_rho;
+  const T dxu = -hw * (T(2) * c200 - c020 - c002) - T(0.5) * inv_rho * (c200 + c020 + c002 - k000);
+  const T dyv = fmat(T(3) * hw, c200 - c020, dxu);
+  const T dzw = fmat(T(3) * hw, c200 - c002, dxu);
+  const T om1 = T(1) - w;
+  const T s110 = om1 * c110;
+  const T s101 = om1 * c101;
+  const T s011 = om1 * c011;
+  const T ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
+  const T g = T(3) * rho * (T(1) - T(0.5) * w);
+  const T ea = om1 * (c200 - c020) - g * (ux2 * dxu - uy2 * dyv);
+  const T eb = om1 * (c200 - c002) - g * (ux2 * dxu - uz2 * dzw);
+  const T ec = k000 - T(1.5) * rho * (ux2 * dxu + uy2 * dyv + uz2 * dzw);
+  const T s200 = T(scalar_t<T>(1) / scalar_t<T>(3)) * (ea + eb + ec);
+  const T s020 = T(scalar_t<T>(1) / scalar_t<T>(3)) * (eb - T(2) * ea + ec);
+  const T s002 = T(scalar_t<T>(1) / scalar_t<T>(3)) * (ea - T(2) * eb + ec);
+
+  populations_from_cumulants(f, k000, -k100, -k010, -k001, s200, s020, s002, s011, s101, s110, inv_rho, ux, uy, uz);
+}
+
+// Smagorinsky relaxation rate (include/cellFunctions.h:157-198): 1/tau without LES, else
+// 1/tau_LES with tau_LES = tau/2 + sqrt(tau^2 + 18 C_s |Pi_neq| / rho)/2, |Pi_neq| from the
+// second-order central moments.
+template <typename T>
+__device__ __forceinline__ T smagorinsky_omega(const T (&K)[3][3][3], T rho, T inv_rho, const RelaxationT<scalar_t<T>>& rx) {
+  T w = T(rx.omega0);
+  if (rx.cs18 != scalar_t<T>(0)) {
+    const T c200 = K[2][0][0], c020 = K[0][2][0], c002 = K[0][0][2];
+    const T c011 = K[0][1][1], c101 = K[1][0][1], c110 = K[1][1][0];
+    const T third = rho * T(scalar_t<T>(1) / scalar_t<T>(3));
+    const T pxx = c200 - third, pyy = c020 - third, pzz = c002 - third;
+    const T p2 = pxx * pxx + pyy * pyy + pzz * pzz + T(2) * (c011 * c011 + c101 * c101 + c110 * c110);
+    const T p = sqrt(p2);
+    const T tau_les = T(scalar_t<T>(0.5) * rx.tau) + T(0.5) * sqrt(fmat(T(rx.cs18) * inv_rho, p, T(rx.tau2)));
+    w = T(1) / tau_les;
+  }
+  return w;
+}
+
 // Cumulant collision (include/applyCollision.h:6-295) with optional body force
 // (half-force velocity shift of M40Impeller/applyCollisionCustomized.h:6-16).
 // Returns the density.
@@ -244,40 +291,7 @@ __device__ __forceinline__ T collide(T (&f)[27], const RelaxationT<scalar_t<T>>&
     uz = (jz + T(0.5) * gz) * inv_rho;
     transform_about(sum, diff, pm, ux, uy, uz, K);
   }
-  const T k000 = K[0][0][0], k100 = K[1][0][0], k010 = K[0][1][0], k001 = K[0][0][1];
-  const T c200 = K[2][0][0], c020 = K[0][2][0], c002 = K[0][0][2];
-  const T c011 = K[0][1][1], c101 = K[1][0][1], c110 = K[1][1][0];
-
-  // Smagorinsky relaxation rate (include/cellFunctions.h:157-198)
-  T w = T(rx.omega0);
-  if (rx.cs18 != scalar_t<T>(0)) {
-    const T third = rho * T(scalar_t<T>(1) / scalar_t<T>(3));
-    const T pxx = c200 - third, pyy = c020 - third, pzz = c002 - third;
-    const T p2 = pxx * pxx + pyy * pyy + pzz * pzz + T(2) * (c011 * c011 + c101 * c101 + c110 * c110);
-    const T p = sqrt(p2);
-    const T tau_les = T(scalar_t<T>(0.5) * rx.tau) + T(0.5) * sqrt(fmat(T(rx.cs18) * inv_rho, p, T(rx.tau2)));
-    w = T(1) / tau_les;
-  }
-
-  // relaxation of the second-order cumulants (Geier 2015 eqs 55-65)
-  const T hw = T(0.5) * w * inv_rho;
-  const T dxu = -hw * (T(2) * c200 - c020 - c002) - T(0.5) * inv_rho * (c200 + c020 + c002 - k000);
-  const T dyv = fmat(T(3) * hw, c200 - c020, dxu);
-  const T dzw = fmat(T(3) * hw, c200 - c002, dxu);
-  const T om1 = T(1) - w;
-  const T s110 = om1 * c110;
-  const T s101 = om1 * c101;
-  const T s011 = om1 * c011;
-  const T ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
-  const T g = T(3) * rho * (T(1) - T(0.5) * w);
-  const T ea = om1 * (c200 - c020) - g * (ux2 * dxu - uy2 * dyv);
-  const T eb = om1 * (c200 - c002) - g * (ux2 * dxu - uz2 * dzw);
-  const T ec = k000 - T(1.5) * rho * (ux2 * dxu + uy2 * dyv + uz2 * dzw);
-  const T s200 = T(scalar_t<T>(1) / scalar_t<T>(3)) * (ea + eb + ec);
-  const T s020 = T(scalar_t<T>(1) / scalar_t<T>(3)) * (eb - T(2) * ea + ec);
-  const T s002 = T(scalar_t<T>(1) / scalar_t<T>(3)) * (ea - T(2) * eb + ec);
-
-  populations_from_cumulants(f, k000, -k100, -k010, -k001, s200, s020, s002, s011, s101, s110, inv_rho, ux, uy, uz);
+  relax_rebuild(f, K, rho, ux, uy, uz, inv_rho, smagorinsky_omega(K, rho, inv_rho, rx));
   return rho;
 }
 

@@ -46,5 +46,10 @@ struct psl_grid {
   int device = 0;
   bool tiled = false;               // bulk-copy tiled update kernel (N % 128 == 0)
   int batched = 0;                  // member of this many live batches (psl_batch.cu)
+  void* mlp = nullptr;              // learned closure (psl::MlpDevice), or null: Smagorinsky
+  float mlp_width = 1.f;            // filter width fed to the closure
 };
+
+// Launches the update kernel with the learned closure (psl_learned.cu); status as psl_*.
+__attribute__((visibility("hidden"))) int psl_detail_launch_learned(psl_grid* g);
 

@@ -1,0 +1,156 @@
+// C ABI of the learned subgrid closure (include/psl.h, psl_set_sgs_mlp / psl_sgs_mlp_infer)
+// and the launch of the update kernel that fuses it (psl_learned.cuh).
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+
+#include "psl.h"
+#include "psl_internal.h"
+#include "psl_learned.cuh"
+
+using namespace psl;
+
+namespace {
+
+int fail(int code, const std::string& msg) {
+  psl_detail_set_last_error(msg);
+  return code;
+}
+
+#define MLP_CUDA(expr)                                                                                 \
+  do {                                                                                                 \
+    cudaError_t e_ = (expr);                                                                           \
+    if (e_ != cudaSuccess) return fail(PSL_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// FP16 weights in the tensor-core operand layout, FP32 biases and normalisation.
+void pack(const psl_sgs_mlp& m, MlpDevice& d) {
+  std::memset(&d, 0, sizeof(d));
+  auto put = [](__half* base, uint32_t rows, uint32_t r, uint32_t k, float v) {
+    base[mlp_operand_offset(rows, r, k) / 2] = __float2half_rn(v);
+  };
+  for (int r = 0; r < kMlpHidden; ++r) {
+    for (int k = 0; k < kMlpK1; ++k) put(d.w1, kMlpHidden, r, k, k < kMlpIn ? m.w1[r][k] : 0.f);
+    for (int k = 0; k < kMlpHidden; ++k) put(d.w2, kMlpHidden, r, k, m.w2[r][k]);
+  }
+  for (int r = 0; r < kMlpN3; ++r)
+    for (int k = 0; k < kMlpHidden; ++k) put(d.w3, kMlpN3, r, k, r == 0 ? m.w3[k] : 0.f);
+  for (int i = 0; i < kMlpHidden; ++i) {
+    d.b1[i] = m.b1[i];
+    d.b2[i] = m.b2[i];
+  }
+  d.b3 = m.b3;
+  d.out_scale = m.out_scale;
+  for (int i = 0; i < kMlpIn; ++i) {
+    d.in_shift[i] = m.in_shift[i];
+    d.in_scale[i] = m.in_scale[i];
+  }
+}
+
+template <typename S>
+int launch(psl_grid* g) {
+  LearnedParams<S> p;
+  p.ri.base = static_cast<typename S::type*>(g->f);
+  p.ri.n = g->n;
+  for (int q = 0; q < 27; ++q) {
+    p.ri.off[q] = (uint32_t)((size_t)q * g->stride + g->shift[q]);
+    p.ri.lim[q] = g->n - g->shift[q];
+  }
+  p.marker = g->marker;
+  p.given = g->given;
+  p.given_uniform = g->given_uniform;
+  p.rx.tau = 3.f * g->info.nu + 0.5f;
+  p.rx.tau2 = p.rx.tau * p.rx.tau;
+  p.rx.omega0 = 1.f / p.rx.tau;
+  p.rx.cs18 = 18.f * g->cs;
+  p.mlp = static_cast<const MlpDevice*>(g->mlp);
+  p.nu = g->info.nu;
+  p.width = g->mlp_width;
+  p.n = g->n;
+  p.health = g->health;
+  int sms = 0, per_sm = 0;
+  MLP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+  MLP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_learned_kernel<S>, kMlpRows, 0));
+  if (per_sm < 1) return fail(PSL_ERR_CUDA, "learned update: kernel cannot be resident");
+  const unsigned int tiles = (g->n + kMlpRows - 1) / kMlpRows;
+  const unsigned int blocks = std::min<unsigned int>(tiles, (unsigned int)(sms * per_sm));
+  step_learned_kernel<S><<<blocks, kMlpRows, 0, g->stream>>>(p);
+  MLP_CUDA(cudaGetLastError());
+  return PSL_OK;
+}
+
+}  // namespace
+
+int psl_detail_launch_learned(psl_grid* g) {
+  if (27ull * g->stride + g->n >= (1ull << 32)) return fail(PSL_ERR_INVALID, "learned update: grid too large");
+  switch (g->storage) {
+    case kStoreF32: return launch<StoreF32>(g);
+    case kStoreF16: return launch<StoreF16>(g);
+    case kStoreBF16: return launch<StoreBF16>(g);
+    default: return fail(PSL_ERR_INVALID, "learned update: FP64 storage is for oracle runs only");
+  }
+}
+
+int psl_set_sgs_mlp(psl_grid* g, const psl_sgs_mlp* mlp, float filter_width) {
+  if (!g) return fail(PSL_ERR_INVALID, "psl_set_sgs_mlp: null grid");
+  DeviceGuard dg(g->device);
+  if (!mlp) {
+    if (g->mlp) {
+      MLP_CUDA(cudaStreamSynchronize(g->stream));
+      cudaFree(g->mlp);
+      g->mlp = nullptr;
+    }
+    return PSL_OK;
+  }
+  if (g->storage == kStoreF64) return fail(PSL_ERR_INVALID, "psl_set_sgs_mlp: FP64 storage is for oracle runs only");
+  MlpDevice host;
+  pack(*mlp, host);
+  if (!g->mlp) {
+    cudaError_t e = cudaMalloc(&g->mlp, sizeof(MlpDevice));
+    if (e != cudaSuccess) {
+      g->mlp = nullptr;
+      cudaGetLastError();
+      return fail(PSL_ERR_NOMEM, std::string("psl_set_sgs_mlp: ") + cudaGetErrorString(e));
+    }
+  }
+  MLP_CUDA(cudaMemcpyAsync(g->mlp, &host, sizeof(MlpDevice), cudaMemcpyHostToDevice, g->stream));
+  MLP_CUDA(cudaStreamSynchronize(g->stream));
+  g->mlp_width = filter_width;
+  return PSL_OK;
+}
+
+int psl_sgs_mlp_infer(const psl_sgs_mlp* mlp, const float* features, int count, float* nu_t) {
+  if (!mlp || !features || !nu_t || count <= 0) return fail(PSL_ERR_INVALID, "psl_sgs_mlp_infer: bad argument");
+  int ndev = 0;
+  MLP_CUDA(cudaGetDeviceCount(&ndev));
+  if (ndev <= 0) return fail(PSL_ERR_CUDA, "psl_sgs_mlp_infer: no CUDA device");
+  MlpDevice host;
+  pack(*mlp, host);
+  MlpDevice* dm = nullptr;
+  float *dx = nullptr, *dy = nullptr;
+  unsigned int* dh = nullptr;
+  cudaError_t e = cudaMalloc(&dm, sizeof(MlpDevice));
+  if (e == cudaSuccess) e = cudaMalloc(&dx, (size_t)count * kMlpIn * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dy, (size_t)count * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dh, sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemset(dh, 0, sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemcpy(dm, &host, sizeof(MlpDevice), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dx, features, (size_t)count * kMlpIn * sizeof(float), cudaMemcpyHostToDevice);
+  unsigned int health = 0;
+  if (e == cudaSuccess) {
+    mlp_infer_kernel<<<(count + kMlpRows - 1) / kMlpRows, kMlpRows>>>(dm, dx, count, dy, dh);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(nu_t, dy, (size_t)count * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(&health, dh, sizeof(unsigned int), cudaMemcpyDeviceToHost);
+  cudaFree(dm);
+  cudaFree(dx);
+  cudaFree(dy);
+  cudaFree(dh);
+  if (e != cudaSuccess) return fail(PSL_ERR_CUDA, std::string("psl_sgs_mlp_infer: ") + cudaGetErrorString(e));
+  if (health) return fail(PSL_ERR_STATE, "psl_sgs_mlp_infer: a tensor-core wait timed out");
+  return PSL_OK;
+}

@@ -103,6 +103,9 @@ int psl_set_smagorinsky(psl_grid* grid, float cs);
 int psl_fill_equilibrium_sphere(psl_grid* grid, const psl_sphere_case* sc);
 /* fillEquilibriumFromFunction with a uniform (rho, u). */
 int psl_fill_equilibrium_uniform(psl_grid* grid, float rho, float ux, float uy, float uz);
+/* fillEquilibriumFromFunction with a field hook: rho_u is a host array of four
+ * logical-order planes [4][N] (rho, ux, uy, uz). */
+int psl_fill_equilibrium_field(psl_grid* grid, const float* rho_u);
 /* applyStreaming (applyStreaming.h:11-31): updates the 27 periodic shifts; no kernel. */
 int psl_apply_streaming(psl_grid* grid);
 /* applyLocalCellUpdate (applyLocalCellUpdate.h:1-74): the fused gather / boundary /
@@ -170,6 +173,37 @@ int psl_set_sgs_mlp(psl_grid* grid, const psl_sgs_mlp* mlp, float filter_width);
 /* The closure alone on host features (count x 10 raw features) -> nu_t (count floats),
  * through the same tensor-core device code (parity tests). */
 int psl_sgs_mlp_infer(const psl_sgs_mlp* mlp, const float* features, int count, float* nu_t);
+
+/* ---- training of the closure (CUDA kernels; samples stay on the device) ----
+ * Samples are raw 10-feature rows with an eddy-viscosity target.  The loss is the mean of
+ * (softplus(z) - target/out_scale)^2 over a batch; the normalisation (in_shift, in_scale,
+ * out_scale) is part of the parameters and is not trained. */
+typedef struct psl_sgs_trainer psl_sgs_trainer;
+int psl_sgs_trainer_create(long long capacity, psl_sgs_trainer** out);
+int psl_sgs_trainer_destroy(psl_sgs_trainer* trainer);
+int psl_sgs_trainer_clear(psl_sgs_trainer* trainer);
+int psl_sgs_trainer_count(const psl_sgs_trainer* trainer, long long* count);
+/* Append n host samples (features n x 10, targets n). */
+int psl_sgs_trainer_add_samples(psl_sgs_trainer* trainer, const float* features, const float* targets, long long n);
+/* Append samples box-filtered 2x from a fine periodic box: `fine` is (2M+1) x (2M+1) x 2M
+ * cells (x/y duplicated faces of applyBCPeriodicX/Y, z periodic through the shift); coarse
+ * cell id (row-major, x fastest) is taken when id % stride == phase % stride.  Features are
+ * those of the 2:1-averaged, fine-to-coarse rescaled populations; the target is
+ * max(0, -tau^d : S / (2 S : S)) with tau the subfilter stress of the 8 children and S the
+ * strain rate of the filtered velocity (coarse lattice units). */
+int psl_sgs_trainer_add_filtered(psl_sgs_trainer* trainer, psl_grid* fine, int M, int stride, unsigned int phase);
+int psl_sgs_trainer_get_samples(psl_sgs_trainer* trainer, long long first, long long n, float* features,
+                                float* targets);
+int psl_sgs_trainer_set_params(psl_sgs_trainer* trainer, const psl_sgs_mlp* mlp); /* also resets Adam */
+int psl_sgs_trainer_get_params(psl_sgs_trainer* trainer, psl_sgs_mlp* mlp);
+/* Mean loss over samples [first, first + count) and its gradient (w1..b3 fields of *grad;
+ * the normalisation fields are zero), with the current parameters. */
+int psl_sgs_trainer_gradient(psl_sgs_trainer* trainer, long long first, long long count, psl_sgs_mlp* grad,
+                             double* loss);
+/* `steps` Adam steps (beta 0.9 / 0.999) on random batches of `batch` samples; *last_loss
+ * is the mean loss of the last batch (before its update). */
+int psl_sgs_trainer_train(psl_sgs_trainer* trainer, int steps, int batch, float lr, unsigned int seed,
+                          double* last_loss);
 
 /* ---- batched form ----
  * Many independent single-level grids (e.g. sphere cases of different sizes and Reynolds

@@ -114,3 +114,41 @@ def random_params(seed: int, scale: float = 0.3) -> dict:
     p["in_scale"] = np.abs(rng.normal(300.0, 50.0, 10))
     p["out_scale"] = np.float64(0.01)
     return p
+
+
+def filtered_samples(fine_f: np.ndarray, M: int, rescale_f2c) -> tuple:
+    """Training samples of a fine periodic box as the library's filter defines them.
+
+    fine_f: logical-order populations [27, N] of the (2M+1) x (2M+1) x 2M fine box;
+    rescale_f2c(f27) -> f27: the fine-to-coarse moment rescaling.  Returns (features
+    [M^3, 10], targets [M^3]) for coarse cells in row-major order (x fastest)."""
+    F = 2 * M
+    f = np.asarray(fine_f, dtype=np.float64).reshape(27, F, F + 1, F + 1)[:, :, :F, :F]  # [q, z, y, x]
+    rho = f.sum(0)
+    u = np.stack([(CX[:, None, None, None] * f).sum(0), (CY[:, None, None, None] * f).sum(0),
+                  (CZ[:, None, None, None] * f).sum(0)]) / rho
+
+    def filt(a):
+        return a.reshape(a.shape[:-3] + (M, 2, M, 2, M, 2)).mean(axis=(-5, -3, -1))
+
+    fbar = filt(f).reshape(27, -1)
+    fc = np.stack([rescale_f2c(fbar[:, i].astype(np.float32)) for i in range(fbar.shape[1])], axis=1)
+    x = features(fc, 1.0)
+    ub = np.stack([(CX[:, None] * fc).sum(0), (CY[:, None] * fc).sum(0), (CZ[:, None] * fc).sum(0)]) / fc.sum(0)
+    ub = ub.reshape(3, M, M, M)
+    pairs = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+    tau = {ab: filt(u[ab[0]] * u[ab[1]]) - ub[ab[0]] * ub[ab[1]] for ab in pairs}
+    tr = (tau[(0, 0)] + tau[(1, 1)] + tau[(2, 2)]) / 3.0
+    T = np.empty((3, 3, M, M, M))
+    for (a, b), v in tau.items():
+        T[a, b] = T[b, a] = v - (tr if a == b else 0.0)
+    axis_of = {0: 2, 1: 1, 2: 0}  # spatial array axis of x, y, z
+    g = np.empty((3, 3, M, M, M))  # g[a][b] = d u_b / d x_a
+    for a in range(3):
+        for b in range(3):
+            g[a, b] = 0.5 * (np.roll(ub[b], -1, axis=axis_of[a]) - np.roll(ub[b], 1, axis=axis_of[a]))
+    S = 0.5 * (g + g.transpose(1, 0, 2, 3, 4))
+    ts = (T * S).sum((0, 1))
+    ss = (S * S).sum((0, 1))
+    target = np.maximum(0.0, -ts / (2.0 * ss + 1e-30))
+    return x, target.reshape(-1)

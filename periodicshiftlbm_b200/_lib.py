@@ -104,6 +104,22 @@ _SIGNATURES = {
     "psl_get_macroscopic": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_set_sgs_mlp": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PslSgsMlp), ctypes.c_float]),
     "psl_sgs_mlp_infer": (ctypes.c_int, [ctypes.POINTER(PslSgsMlp), ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "psl_fill_equilibrium_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "psl_sgs_trainer_create": (ctypes.c_int, [ctypes.c_longlong, ctypes.POINTER(ctypes.c_void_p)]),
+    "psl_sgs_trainer_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "psl_sgs_trainer_clear": (ctypes.c_int, [ctypes.c_void_p]),
+    "psl_sgs_trainer_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
+    "psl_sgs_trainer_add_samples": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong]),
+    "psl_sgs_trainer_add_filtered": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_uint]),
+    "psl_sgs_trainer_get_samples": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong,
+                                                   ctypes.c_void_p, ctypes.c_void_p]),
+    "psl_sgs_trainer_set_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PslSgsMlp)]),
+    "psl_sgs_trainer_get_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PslSgsMlp)]),
+    "psl_sgs_trainer_gradient": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong,
+                                                ctypes.POINTER(PslSgsMlp), ctypes.POINTER(ctypes.c_double)]),
+    "psl_sgs_trainer_train": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint,
+                                             ctypes.POINTER(ctypes.c_double)]),
     "psl_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "psl_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "psl_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

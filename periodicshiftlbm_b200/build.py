@@ -26,7 +26,8 @@ NVCC_FLAGS = [
     "-shared", "-Xcompiler", "-fPIC",
 ]
 SOURCES = [os.path.join(CSRC, "psl_capi.cu"), os.path.join(CSRC, "psl_noalloc.cu"), os.path.join(CSRC, "psl_batch.cu"),
-           os.path.join(CSRC, "psl_learned.cu")]
+           os.path.join(CSRC, "psl_learned.cu"),
+           os.path.join(CSRC, "psl_train.cu")]
 
 
 def _nvcc() -> str:

@@ -276,6 +276,26 @@ int psl_fill_equilibrium_uniform(psl_grid* g, float rho, float ux, float uy, flo
   return fill_eq(g, c);
 }
 
+int psl_fill_equilibrium_field(psl_grid* g, const float* rho_u) {
+  PSL_CHECK(g && rho_u, PSL_ERR_INVALID, "psl_fill_equilibrium_field: null argument");
+  DeviceGuard dg(g->device);
+  float* tmp = nullptr;
+  PSL_CUDA(cudaMalloc(&tmp, (size_t)g->n * 4 * sizeof(float)));
+  cudaError_t e = cudaMemcpyAsync(tmp, rho_u, (size_t)g->n * 4 * sizeof(float), cudaMemcpyHostToDevice, g->stream);
+  if (e == cudaSuccess) {
+    with_storage(g->storage, [&](auto s) {
+      using S = decltype(s);
+      fill_equilibrium_field_kernel<S><<<blocks_for(g->n, 256), 256, 0, g->stream>>>(view<S>(g), tmp);
+      return 0;
+    });
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return fail(PSL_ERR_CUDA, std::string("psl_fill_equilibrium_field: ") + cudaGetErrorString(e));
+  return PSL_OK;
+}
+
 int psl_apply_streaming(psl_grid* g) {
   PSL_CHECK(g, PSL_ERR_INVALID, "psl_apply_streaming: null grid");
   const long long nx = g->info.cell_count_x, ny = g->info.cell_count_y, n = g->n;

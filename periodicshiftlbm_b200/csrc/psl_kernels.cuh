@@ -219,6 +219,18 @@ __global__ void fill_equilibrium_kernel(GridView<S> g, Case c, InfoStruct I) {
   store_cell<S>(g, cell, fe);
 }
 
+// fillEquilibrium with a field hook: rho_u holds four logical-order planes (rho, ux, uy, uz).
+template <typename S>
+__global__ void fill_equilibrium_field_kernel(GridView<S> g, const float* __restrict__ rho_u) {
+  const uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= g.n) return;
+  const size_t n = g.n;
+  using T = typename S::calc;
+  T fe[27];
+  equilibrium<T>(rho_u[cell], rho_u[n + cell], rho_u[2 * n + cell], rho_u[3 * n + cell], fe);
+  store_cell<S>(g, cell, fe);
+}
+
 // ------------------------------------------------------------------------------------------
 // periodic x / y fix-up after streaming (include/boundaryConditions/periodicXY.h:11-101):
 // the 9 populations with c_x > 0 of the left face come from the right face, those with

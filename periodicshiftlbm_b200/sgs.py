@@ -48,3 +48,107 @@ def mlp_infer(p: dict, x: np.ndarray) -> np.ndarray:
     m = to_c(p)
     call("psl_sgs_mlp_infer", ctypes.byref(m), x.ctypes.data, x.shape[0], out.ctypes.data)
     return out
+
+
+class Trainer:
+    """psl_sgs_trainer: training samples on the device, CUDA forward/backward kernels and
+    Adam (include/psl.h)."""
+
+    def __init__(self, capacity: int):
+        self._h = ctypes.c_void_p()
+        call("psl_sgs_trainer_create", ctypes.c_longlong(int(capacity)), ctypes.byref(self._h))
+
+    def close(self):
+        if self._h and self._h.value:
+            from . import _lib
+
+            _lib.lib().psl_sgs_trainer_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def count(self) -> int:
+        n = ctypes.c_longlong()
+        call("psl_sgs_trainer_count", self._h, ctypes.byref(n))
+        return n.value
+
+    def clear(self):
+        call("psl_sgs_trainer_clear", self._h)
+
+    def add_samples(self, x: np.ndarray, t: np.ndarray):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        call("psl_sgs_trainer_add_samples", self._h, x.ctypes.data, t.ctypes.data, ctypes.c_longlong(x.shape[0]))
+
+    def add_filtered(self, fine_grid, M: int, stride: int = 1, phase: int = 0):
+        call("psl_sgs_trainer_add_filtered", self._h, fine_grid.handle, int(M), int(stride), ctypes.c_uint(phase))
+
+    def samples(self, first: int = 0, n: int | None = None):
+        n = self.count - first if n is None else n
+        x = np.empty((n, 10), dtype=np.float32)
+        t = np.empty(n, dtype=np.float32)
+        call("psl_sgs_trainer_get_samples", self._h, ctypes.c_longlong(first), ctypes.c_longlong(n), x.ctypes.data,
+             t.ctypes.data)
+        return x, t
+
+    @property
+    def params(self) -> dict:
+        m = PslSgsMlp()
+        call("psl_sgs_trainer_get_params", self._h, ctypes.byref(m))
+        return from_c(m)
+
+    @params.setter
+    def params(self, p: dict):
+        m = to_c(p)
+        call("psl_sgs_trainer_set_params", self._h, ctypes.byref(m))
+
+    def gradient(self, first: int, count: int):
+        """(mean loss, gradient dict w1..b3) over samples [first, first + count)."""
+        g = PslSgsMlp()
+        loss = ctypes.c_double()
+        call("psl_sgs_trainer_gradient", self._h, ctypes.c_longlong(first), ctypes.c_longlong(count), ctypes.byref(g),
+             ctypes.byref(loss))
+        d = from_c(g)
+        return loss.value, {k: d[k] for k in ("w1", "b1", "w2", "b2", "w3", "b3")}
+
+    def train(self, steps: int, batch: int = 65536, lr: float = 1e-3, seed: int = 1) -> float:
+        loss = ctypes.c_double()
+        call("psl_sgs_trainer_train", self._h, int(steps), int(batch), ctypes.c_float(lr), ctypes.c_uint(seed),
+             ctypes.byref(loss))
+        return loss.value
+
+
+def init_params(x: np.ndarray, t: np.ndarray, seed: int = 0) -> dict:
+    """He-initialised weights with the normalisation taken from the samples: in_shift and
+    in_scale standardise each feature (a constant feature keeps scale 1), out_scale is the
+    mean target."""
+    rng = np.random.default_rng(seed)
+    x = np.asarray(x, dtype=np.float64)
+    mean = x.mean(0)
+    std = x.std(0)
+    scale = np.where(std > 1e-12 * np.maximum(np.abs(mean), 1e-30), 1.0 / np.maximum(std, 1e-30), 1.0)
+    return {
+        "w1": rng.normal(0.0, np.sqrt(2.0 / 10), (32, 10)),
+        "b1": np.zeros(32),
+        "w2": rng.normal(0.0, np.sqrt(2.0 / 32), (32, 32)),
+        "b2": np.zeros(32),
+        "w3": rng.normal(0.0, np.sqrt(1.0 / 32), 32),
+        "b3": np.float64(0.0),
+        "in_shift": mean,
+        "in_scale": scale,
+        "out_scale": np.float64(max(float(np.mean(t)), 1e-12)),
+    }
+
+
+def smagorinsky_nu_t(x: np.ndarray, nu: float, cs: float) -> np.ndarray:
+    """Eddy viscosity of the Smagorinsky rate (cellFunctions.h:157-198) from the same
+    features: tau_LES = tau/2 + sqrt(tau^2 + 18 C_s |Pi|)/2 with |Pi| = x[:, 7] (per unit
+    density), nu_t = (tau_LES - 1/2)/3 - nu."""
+    tau = 3.0 * nu + 0.5
+    tau_les = 0.5 * tau + 0.5 * np.sqrt(tau * tau + 18.0 * cs * np.asarray(x, dtype=np.float64)[:, 7])
+    return (tau_les - 0.5) / 3.0 - nu

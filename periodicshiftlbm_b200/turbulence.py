@@ -46,23 +46,35 @@ def box_grid(M: int, nu: float, storage: str = "f32", cs: float = 0.0) -> GridSt
 
 
 def initial_velocity(M: int, seed: int, u_rms: float = 0.04, k0: float = 4.0) -> np.ndarray:
-    """[3, z, y, x] float32 velocity on an M^3 periodic lattice."""
+    """[3, z, y, x] float32 velocity on an M^3 periodic lattice (component 0 along x)."""
+    try:
+        from scipy import fft as sfft
+
+        irfftn = lambda a: sfft.irfftn(a, s=(M, M, M), axes=(1, 2, 3), workers=-1)  # noqa: E731
+    except ImportError:  # pragma: no cover
+        irfftn = lambda a: np.fft.irfftn(a, s=(M, M, M), axes=(1, 2, 3))  # noqa: E731
     rng = np.random.default_rng(seed)
-    kz = np.fft.fftfreq(M, 1.0 / M)[:, None, None]
-    ky = np.fft.fftfreq(M, 1.0 / M)[None, :, None]
-    kx = np.fft.rfftfreq(M, 1.0 / M)[None, None, :]
     shape = (M, M, M // 2 + 1)
-    k2 = (kx * kx + ky * ky + kz * kz) * np.ones(shape)
+    kz = np.fft.fftfreq(M, 1.0 / M).astype(np.float32)[:, None, None]
+    ky = np.fft.fftfreq(M, 1.0 / M).astype(np.float32)[None, :, None]
+    kx = np.fft.rfftfreq(M, 1.0 / M).astype(np.float32)[None, None, :]
+    a = np.empty((3,) + shape, dtype=np.complex64)
+    for c in range(3):
+        a[c].real = rng.standard_normal(shape, dtype=np.float32)
+        a[c].imag = rng.standard_normal(shape, dtype=np.float32)
+    k2 = kx * kx + ky * ky + kz * kz
+    safe = np.where(k2 > 0, k2, 1.0).astype(np.float32)
+    proj = (a[0] * kx + a[1] * ky + a[2] * kz) / safe
+    a[0] -= kx * proj  # divergence-free: k . a = 0
+    a[1] -= ky * proj
+    a[2] -= kz * proj
+    del proj
     k = np.sqrt(k2)
-    a = rng.normal(size=(3,) + shape) + 1j * rng.normal(size=(3,) + shape)
-    kvec = np.stack([np.broadcast_to(kx, shape), np.broadcast_to(ky, shape), np.broadcast_to(kz, shape)])
-    with np.errstate(invalid="ignore", divide="ignore"):
-        proj = (a * kvec).sum(0) / np.where(k2 > 0, k2, 1.0)
-        a = a - kvec * proj[None]  # divergence-free: k . a = 0
-        amp = np.where(k > 0, np.sqrt(k ** 4 * np.exp(-2.0 * (k / k0) ** 2) / (4.0 * np.pi * np.maximum(k2, 1.0))), 0.0)
-        norm = np.sqrt((np.abs(a) ** 2).sum(0))
-        a = a * np.where(norm > 0, amp / np.maximum(norm, 1e-30), 0.0)[None]
-    u = np.fft.irfftn(a, s=(M, M, M), axes=(1, 2, 3))  # order (x, y, z) components along axis 0
+    amp = np.where(k2 > 0, np.sqrt(k2 * k2 * np.exp(-2.0 * (k / k0) ** 2) / (4.0 * np.pi * safe)), 0.0).astype(np.float32)
+    norm = np.sqrt((np.abs(a) ** 2).sum(0))
+    a *= np.where(norm > 0, amp / np.maximum(norm, 1e-30), 0.0).astype(np.float32)[None]
+    del norm, amp, k
+    u = irfftn(a).astype(np.float64)
     u *= u_rms / np.sqrt(np.mean(u ** 2))
     return u.astype(np.float32)
 

@@ -126,6 +126,27 @@ int psl_update_grid(psl_grid** grids, int levels, int level);
  * drag (x), force[1..2] the y and z components. */
 int psl_sphere_force(psl_grid* grid, const psl_sphere_case* sc, double* force3);
 
+/* Torque (r x F, r = cell centre - point3, physical units of the grid) and force of the
+ * momentum exchange summed over the solid cells of the box [lo3, hi3), FP64.  Counterpart
+ * of getTorque (M35Full/m35Main.cu:176-260, which sums -F_x y + F_y x of forced-velocity
+ * cells through its case's forcing hook) for bounce-back bodies; force3 may be NULL. */
+int psl_torque(psl_grid* grid, const int* lo3, const int* hi3, const float* point3, double* torque3, double* force3);
+
+/* getFlowReportGeneral (flowReportFunctions.h:2-251) over a grid hierarchy (grids[0]
+ * coarsest): section plane `plane` at finest-grid index `cut_index`, cropped to the physical
+ * bounds {xmin, ymin, zmin, xmax, ymax, zmax}; mean velocity and density over the non-solid
+ * pixels and their area (FlowReportStruct, include/types.h:123), summed in FP64. */
+#define PSL_PLANE_XY 0
+#define PSL_PLANE_ZY 1
+#define PSL_PLANE_ZX 2
+typedef struct psl_flow_report {
+  double ux, uy, uz;
+  double rho;
+  double area; /* pixel count x (target cell size)^2, physical units (mm^2 in the reference) */
+} psl_flow_report;
+int psl_get_flow_report(psl_grid* const* grids, int levels, int plane, int cut_index, const float* bounds6,
+                        psl_flow_report* report);
+
 /* Momentum-exchange force over the solid cells of the box [box_lo3, box_hi3), FP64, on
  * caller-owned buffers, allocating no device memory.  No counterpart in the reference.
  * For callers that cannot call cudaMalloc when they need the force: step loops running

@@ -17,7 +17,9 @@ from .grid import (  # noqa: F401
     drag_coefficient,
     fillEquilibriumFromFunction,
     getSphereDrag,
+    getFlowReport,
     getSphereForce,
+    getTorque,
     setGivenRhoUxUyUz,
     setSmagorinskyConstant,
     setSphereCase,

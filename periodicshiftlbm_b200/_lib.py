@@ -67,6 +67,11 @@ class PslSgsMlp(ctypes.Structure):
     ]
 
 
+class PslFlowReport(ctypes.Structure):
+    _fields_ = [("ux", ctypes.c_double), ("uy", ctypes.c_double), ("uz", ctypes.c_double), ("rho", ctypes.c_double),
+                ("area", ctypes.c_double)]
+
+
 class PslError(RuntimeError):
     pass
 
@@ -120,6 +125,10 @@ _SIGNATURES = {
                                                 ctypes.POINTER(PslSgsMlp), ctypes.POINTER(ctypes.c_double)]),
     "psl_sgs_trainer_train": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint,
                                              ctypes.POINTER(ctypes.c_double)]),
+    "psl_torque": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                  ctypes.c_void_p]),
+    "psl_get_flow_report": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_void_p, ctypes.POINTER(PslFlowReport)]),
     "psl_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "psl_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "psl_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

@@ -27,7 +27,8 @@ NVCC_FLAGS = [
 ]
 SOURCES = [os.path.join(CSRC, "psl_capi.cu"), os.path.join(CSRC, "psl_noalloc.cu"), os.path.join(CSRC, "psl_batch.cu"),
            os.path.join(CSRC, "psl_learned.cu"),
-           os.path.join(CSRC, "psl_train.cu")]
+           os.path.join(CSRC, "psl_train.cu"),
+           os.path.join(CSRC, "psl_reports.cu")]
 
 
 def _nvcc() -> str:

@@ -271,6 +271,32 @@ def getSphereDrag(grid: GridStruct, case: SphereCase) -> float:
     return float(getSphereForce(grid, case)[0])
 
 
+def getTorque(grid: GridStruct, lo, hi, point) -> tuple:
+    """(torque[3], force[3]) of the momentum exchange on the solid cells of the box
+    [lo, hi) about `point` (psl_torque; getTorque, M35Full/m35Main.cu:176-260)."""
+    lo = np.ascontiguousarray(lo, dtype=np.int32)
+    hi = np.ascontiguousarray(hi, dtype=np.int32)
+    pt = np.ascontiguousarray(point, dtype=np.float32)
+    t = np.zeros(3)
+    f = np.zeros(3)
+    call("psl_torque", grid.handle, lo.ctypes.data, hi.ctypes.data, pt.ctypes.data, t.ctypes.data, f.ctypes.data)
+    return t, f
+
+
+PLANES = {"XY": 0, "ZY": 1, "ZX": 2}
+
+
+def getFlowReport(grids, plane: str, cut_index: int, bounds) -> dict:
+    """getFlowReportGeneral (flowReportFunctions.h:2-251) over the grid hierarchy `grids`
+    (coarsest first): mean ux, uy, uz, rho and the area of the section at finest index
+    `cut_index`, bounds = (xmin, ymin, zmin, xmax, ymax, zmax) physical."""
+    arr = (ctypes.c_void_p * len(grids))(*[g.handle.value for g in grids])
+    b = np.ascontiguousarray(bounds, dtype=np.float32)
+    r = _lib.PslFlowReport()
+    call("psl_get_flow_report", arr, len(grids), PLANES[plane], int(cut_index), b.ctypes.data, ctypes.byref(r))
+    return {"ux": r.ux, "uy": r.uy, "uz": r.uz, "rho": r.rho, "area": r.area}
+
+
 def drag_coefficient(drag_lattice: float, grid_info: InfoStruct, case: SphereCase, coarse_res: float = 1.0) -> float:
     """Cd = F / (rho U^2 pi D^2 / 8) with F and U in the units of the grid the force was
     summed on (the reference converts both to physical units: the factors cancel)."""

@@ -50,6 +50,8 @@ def parse():
                    help="linear scale of the config-2 geometry (0.5: a 256x128x128 case for ncu captures)")
     p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
     p.add_argument("--form", default="single", choices=["single", "batch"])
+    p.add_argument("--sgs", default="smagorinsky", choices=["smagorinsky", "mlp"],
+                   help="mlp: the learned closure trained on decaying turbulence (packaged weights)")
     p.add_argument("--batch-cases", type=int, default=64)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-steps", type=int, default=2)
@@ -146,9 +148,9 @@ def hbm_peak():
 
 
 def ncu_traffic(kernel: str, storage: str):
-    """dram bytes read+written per launch of the coarse step kernel from the committed ncu
-    summary (profiles/step_kernel_<storage>_sphere512.md), or None."""
-    path = os.path.join(REPO, "profiles", f"step_kernel_{storage}_sphere512.md")
+    """dram bytes read+written per launch of the coarse update kernel from the committed
+    ncu summary (profiles/<kernel>_<storage>_sphere512.md), or None."""
+    path = os.path.join(REPO, "profiles", f"{kernel}_{storage}_sphere512.md")
     if not os.path.exists(path):
         return None
     m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
@@ -183,6 +185,12 @@ def run_native(args):
     grids, case = make_sphere_grids(cfg, storage=args.storage)
     for g in grids:
         g.set_stream(stream.cuda_stream)
+    if args.sgs == "mlp":
+        from periodicshiftlbm_b200.sgs import load_params, set_sgs_mlp
+
+        closure = load_params()
+        for g in grids:
+            set_sgs_mlp(g, closure, g.Info.res / grids[0].Info.res)
     torch.cuda.synchronize()
     levels = len(grids)
     ev = {"coarse": [], "fine": []}
@@ -296,19 +304,20 @@ def run_native(args):
             "storage": args.storage,
             "updates_per_step": updates,
             "reference_formula_updates_per_step": cfg.reference_updates_per_step(),
-            "collision": "cumulant + Smagorinsky" if cfg.smagorinsky else "cumulant",
+            "collision": ("cumulant + learned MLP closure (tcgen05)" if args.sgs == "mlp" else
+                          "cumulant + Smagorinsky" if cfg.smagorinsky else "cumulant"),
             "l2": "inputs larger than L2 (no flush)" if cfg.refine else "state fits partly in L2",
             "parallelism": f"replicas x{world}",
         },
         "roofline": {
             "bound": "hbm",
-            "kernel": "step_kernel (coarse grid)",
+            "kernel": "step_learned_kernel (coarse grid)" if args.sgs == "mlp" else "step_kernel (coarse grid)",
             "achieved": round(achieved, 1),
             "peak": peak,
             "peak_kind": peak_kind,
             "unit": "GB/s",
             "frac": round(achieved / peak, 4),
-            "traffic": ncu_traffic("step_kernel", args.storage),
+            "traffic": ncu_traffic("step_learned_kernel" if args.sgs == "mlp" else "step_kernel", args.storage),
             "algorithmic_bytes_per_launch": coarse_bytes,
             "launch_ms": round(coarse_ms, 4),
             "fine_launch_ms": round(fine_ms, 4) if fine_ms else None,

@@ -55,6 +55,19 @@ static GridView<S> view(const psl_grid* g) {
   return v;
 }
 
+// Base pointer + 32-bit row offsets of a grid (needs 27 * stride + N < 2^32).
+template <typename S>
+static RowIndex<S> row_index(const psl_grid* g) {
+  RowIndex<S> r;
+  r.base = static_cast<typename S::type*>(g->f);
+  r.n = g->n;
+  for (int q = 0; q < 27; ++q) {
+    r.off[q] = (uint32_t)((size_t)q * g->stride + g->shift[q]);
+    r.lim[q] = g->n - g->shift[q];
+  }
+  return r;
+}
+
 static InfoStruct hook_info(const psl_grid* g) {
   InfoStruct I;
   I.gridID = (float)g->info.grid_id;
@@ -393,8 +406,8 @@ static int launch_coarse_fine(psl_grid* c, psl_grid* f) {
   const int a = C.i_subgrid_end - C.i_subgrid_start, b = C.j_subgrid_end - C.j_subgrid_start,
             cc = C.k_subgrid_end - C.k_subgrid_start;
   CoarseFineParams<S> p;
-  p.c = view<S>(c);
-  p.f = view<S>(f);
+  p.c = row_index<S>(c);
+  p.f = row_index<S>(f);
   p.cnx = C.cell_count_x;
   p.cny = C.cell_count_y;
   p.cnz = C.cell_count_z;
@@ -441,6 +454,8 @@ int psl_apply_coarse_fine_grid_communication(psl_grid* c, psl_grid* f) {
   PSL_CHECK(F.cell_count_x == 2 * a && F.cell_count_y == 2 * b && F.cell_count_z == 2 * cc, PSL_ERR_INVALID,
             "coarse/fine: fine grid is not twice the refinement block");
   PSL_CHECK(c->device == f->device, PSL_ERR_INVALID, "coarse/fine: grids on different devices");
+  PSL_CHECK(27ull * c->stride + c->n < (1ull << 32) && 27ull * f->stride + f->n < (1ull << 32), PSL_ERR_INVALID,
+            "coarse/fine: grid too large for 32-bit row offsets");
   DeviceGuard dg(c->device);
   return with_storage(c->storage, [&](auto s) { return launch_coarse_fine<decltype(s)>(c, f); });
 }

@@ -279,8 +279,8 @@ __global__ void periodic_kernel(GridView<S> g, int nx, int ny, int nz) {
 // ------------------------------------------------------------------------------------------
 template <typename S>
 struct CoarseFineParams {
-  GridView<S> c;
-  GridView<S> f;
+  RowIndex<S> c;
+  RowIndex<S> f;
   int cnx, cny, cnz;
   int iS, jS, kS, iE, jE, kE;
   int fnx, fny, fnz;
@@ -324,12 +324,12 @@ __device__ __forceinline__ void grid_barrier(unsigned int* counter, unsigned int
 // line before the barrier in this launch, and L1 starts empty for every launch, so no
 // stale copy of a restricted ring cell can be hit.
 template <typename S>
-__device__ __forceinline__ typename S::calc load_pop(const GridView<S>& g, int q, uint32_t cell) {
-  return S::load_q(g.fq[q] + shifted(cell, g.shift[q], g.n), q);
+__device__ __forceinline__ typename S::calc load_pop(const RowIndex<S>& r, int q, uint32_t cell) {
+  return S::load_q(r.base + (cell + r.off[q] - (cell >= r.lim[q] ? r.n : 0u)), q);
 }
 template <typename S>
-__device__ __forceinline__ void store_pop(const GridView<S>& g, int q, uint32_t cell, typename S::calc v) {
-  S::store_q(g.fq[q] + shifted(cell, g.shift[q], g.n), v, q);
+__device__ __forceinline__ void store_pop(const RowIndex<S>& r, int q, uint32_t cell, typename S::calc v) {
+  S::store_q(r.base + (cell + r.off[q] - (cell >= r.lim[q] ? r.n : 0u)), v, q);
 }
 
 // Work items are dealt out in warp-sized chunks, consecutive chunks to consecutive blocks,
@@ -344,6 +344,22 @@ constexpr int kCoarseFineThreads = 128;
 template <typename S>
 __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const __grid_constant__ CoarseFineParams<S> p) {
   using T = typename S::calc;
+  // The row offsets of both grids are read from shared memory inside the item loops (kept
+  // as kernel parameters, the compiler holds all of them in registers across iterations).
+  __shared__ RowIndex<S> rc, rf;
+  if (threadIdx.x < 27) {
+    rc.off[threadIdx.x] = p.c.off[threadIdx.x];
+    rc.lim[threadIdx.x] = p.c.lim[threadIdx.x];
+    rf.off[threadIdx.x] = p.f.off[threadIdx.x];
+    rf.lim[threadIdx.x] = p.f.lim[threadIdx.x];
+  }
+  if (threadIdx.x == 0) {
+    rc.base = p.c.base;
+    rc.n = p.c.n;
+    rf.base = p.f.base;
+    rf.n = p.f.n;
+  }
+  __syncthreads();
   // ---------------- phase 1: restriction ----------------
   {
     const int a = p.iE - p.iS - 2, b = p.jE - p.jS - 2, c = p.kE - p.kS - 2;  // ring box extents
@@ -380,14 +396,14 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
           for (int di = 0; di <= 1; ++di) {
             const uint32_t fc = ((uint32_t)(fk + dk) * p.fny + (fj + dj)) * p.fnx + (fi + di);
 #pragma unroll
-            for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], load_pop(p.f, q, fc));
+            for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], load_pop(rf, q, fc));
           }
 #pragma unroll
       for (int q = 0; q < 27; ++q) f[q] = f[q] * T(0.125);
       rescale(f, false);
       const uint32_t cc = ((uint32_t)k * p.cny + j) * p.cnx + i;
 #pragma unroll
-      for (int q = 0; q < 27; ++q) store_pop(p.c, q, cc, f[q]);
+      for (int q = 0; q < 27; ++q) store_pop(rc, q, cc, f[q]);
     }
   }
   grid_barrier(p.barrier, p.nblocks, p.error);
@@ -433,7 +449,7 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
     T f[27];
     const uint32_t pc = ((uint32_t)kc * p.cny + jc) * p.cnx + ic;
 #pragma unroll
-    for (int q = 0; q < 27; ++q) f[q] = load_pop(p.c, q, pc);
+    for (int q = 0; q < 27; ++q) f[q] = load_pop(rc, q, pc);
     const int cidx[3] = {ic, jc, kc};
     const int cdim[3] = {p.cnx, p.cny, p.cnz};
 #pragma unroll
@@ -449,13 +465,13 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
         const T w = (side == 0 ? inv : -inv) * d[ax];  // exact: powers of two
         const uint32_t nc = ((uint32_t)nb[2] * p.cny + nb[1]) * p.cnx + nb[0];
 #pragma unroll
-        for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], load_pop(p.c, q, nc) * w);
+        for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], load_pop(rc, q, nc) * w);
       }
     }
     rescale(f, true);
 #pragma unroll
     for (int q = 0; q < 27; ++q)
-      if (mask & (1u << q)) store_pop(p.f, q, fcell, f[q]);
+      if (mask & (1u << q)) store_pop(rf, q, fcell, f[q]);
   }
 }
 

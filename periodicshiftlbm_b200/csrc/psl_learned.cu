@@ -26,7 +26,31 @@ int fail(int code, const std::string& msg) {
     if (e_ != cudaSuccess) return fail(PSL_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
-// FP16 weights in the tensor-core operand layout, FP32 biases and normalisation.
+// The grid's closure buffer: the tcgen05 layout followed by the per-warp layout.
+struct MlpBoth {
+  MlpDevice cta;
+  MlpWarp warp;
+};
+
+// Per-warp layout: W[out][in] FP16 rows (padded), FP32 biases and normalisation.
+void pack_warp(const psl_sgs_mlp& m, MlpWarp& d) {
+  std::memset(&d, 0, sizeof(d));
+  for (int o = 0; o < 32; ++o) {
+    for (int k = 0; k < kMlpIn; ++k) d.w1[o * kW1Stride + k] = __float2half_rn(m.w1[o][k]);
+    for (int k = 0; k < 32; ++k) d.w2[o * kW2Stride + k] = __float2half_rn(m.w2[o][k]);
+    d.b1[o] = m.b1[o];
+    d.b2[o] = m.b2[o];
+  }
+  for (int k = 0; k < 32; ++k) d.w3[k] = __float2half_rn(m.w3[k]);  // row 0
+  d.b3 = m.b3;
+  d.out_scale = m.out_scale;
+  for (int i = 0; i < kMlpIn; ++i) {
+    d.in_shift[i] = m.in_shift[i];
+    d.in_scale[i] = m.in_scale[i];
+  }
+}
+
+// FP16 weights in the tcgen05 operand layout, FP32 biases and normalisation.
 void pack(const psl_sgs_mlp& m, MlpDevice& d) {
   std::memset(&d, 0, sizeof(d));
   auto put = [](__half* base, uint32_t rows, uint32_t r, uint32_t k, float v) {
@@ -66,18 +90,29 @@ int launch(psl_grid* g) {
   p.rx.tau2 = p.rx.tau * p.rx.tau;
   p.rx.omega0 = 1.f / p.rx.tau;
   p.rx.cs18 = 18.f * g->cs;
-  p.mlp = static_cast<const MlpDevice*>(g->mlp);
+  p.mlp = &static_cast<const MlpBoth*>(g->mlp)->cta;
+  p.mlpw = &static_cast<const MlpBoth*>(g->mlp)->warp;
   p.nu = g->info.nu;
   p.width = g->mlp_width;
   p.n = g->n;
   p.health = g->health;
+  // PSL_CLOSURE_PATH=tcgen05 selects the CTA-wide tcgen05 evaluation; default per warp
+  const char* path_env = getenv("PSL_CLOSURE_PATH");
+  const bool cta_path = path_env && std::string(path_env) == "tcgen05";
   int sms = 0, per_sm = 0;
   MLP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
-  MLP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_learned_kernel<S>, kMlpRows, 0));
+  if (cta_path)
+    MLP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_learned_kernel<S>, kMlpRows, 0));
+  else
+    MLP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_learned_warp_kernel<S>, kStepThreads, 0));
   if (per_sm < 1) return fail(PSL_ERR_CUDA, "learned update: kernel cannot be resident");
   const unsigned int tiles = (g->n + kMlpRows - 1) / kMlpRows;
   const unsigned int blocks = std::min<unsigned int>(tiles, (unsigned int)(sms * per_sm));
-  step_learned_kernel<S><<<blocks, kMlpRows, 0, g->stream>>>(p);
+  (void)blocks;
+  if (cta_path)
+    step_learned_kernel<S><<<tiles, kMlpRows, 0, g->stream>>>(p);
+  else
+    step_learned_warp_kernel<S><<<(g->n + kStepThreads - 1) / kStepThreads, kStepThreads, 0, g->stream>>>(p);
   MLP_CUDA(cudaGetLastError());
   return PSL_OK;
 }
@@ -106,17 +141,18 @@ int psl_set_sgs_mlp(psl_grid* g, const psl_sgs_mlp* mlp, float filter_width) {
     return PSL_OK;
   }
   if (g->storage == kStoreF64) return fail(PSL_ERR_INVALID, "psl_set_sgs_mlp: FP64 storage is for oracle runs only");
-  MlpDevice host;
-  pack(*mlp, host);
+  MlpBoth host;
+  pack(*mlp, host.cta);
+  pack_warp(*mlp, host.warp);
   if (!g->mlp) {
-    cudaError_t e = cudaMalloc(&g->mlp, sizeof(MlpDevice));
+    cudaError_t e = cudaMalloc(&g->mlp, sizeof(MlpBoth));
     if (e != cudaSuccess) {
       g->mlp = nullptr;
       cudaGetLastError();
       return fail(PSL_ERR_NOMEM, std::string("psl_set_sgs_mlp: ") + cudaGetErrorString(e));
     }
   }
-  MLP_CUDA(cudaMemcpyAsync(g->mlp, &host, sizeof(MlpDevice), cudaMemcpyHostToDevice, g->stream));
+  MLP_CUDA(cudaMemcpyAsync(g->mlp, &host, sizeof(MlpBoth), cudaMemcpyHostToDevice, g->stream));
   MLP_CUDA(cudaStreamSynchronize(g->stream));
   g->mlp_width = filter_width;
   return PSL_OK;

@@ -143,20 +143,17 @@ __device__ __forceinline__ void mlp_tmem_dealloc(uint32_t taddr, uint32_t cols) 
   asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols) : "memory");
 }
 
-// 32 consecutive FP32 columns of this thread's TMEM lane.
-__device__ __forceinline__ void mlp_tmem_load32(uint32_t taddr, float (&v)[32]) {
-  uint32_t r[32];
+// 16 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void mlp_tmem_load16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
-        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 __device__ __forceinline__ float mlp_tmem_load1(uint32_t taddr) {
@@ -209,18 +206,6 @@ __device__ __forceinline__ void mlp_cta_teardown(MlpShared& s) {
   if (threadIdx.x < 32) mlp_tmem_dealloc(s.tmem, kMlpTmemCols);
 }
 
-// Stores 32 FP32 values of row `row` into an operand buffer with `rows` rows (K = 32) as
-// FP16, as four 16-byte chunks.
-__device__ __forceinline__ void mlp_store_row32(unsigned char* buf, uint32_t row, const float (&v)[32]) {
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    __half2 h[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) h[e] = __floats2half2_rn(v[c * 8 + 2 * e], v[c * 8 + 2 * e + 1]);
-    *reinterpret_cast<uint4*>(buf + mlp_operand_offset(kMlpRows, row, c * 8)) = *reinterpret_cast<uint4*>(h);
-  }
-}
-
 // Evaluate the closure for the CTA's 128 cells; every thread of the CTA must call it (the
 // thread's row is threadIdx.x).  `x` holds the thread's raw features.  Returns nu_t, or a
 // negative value when the closure is unavailable (a wait timed out in this launch; the
@@ -248,7 +233,6 @@ __device__ __forceinline__ float mlp_eval(MlpShared& s, const float (&x)[kMlpIn]
     }
   }
   bool ok = !s.failed;
-  float h[32];
   // three layers; A of layer 1 is a1, of layers 2 and 3 a2
 #pragma unroll
   for (int layer = 0; layer < 3; ++layer) {
@@ -283,13 +267,26 @@ __device__ __forceinline__ float mlp_eval(MlpShared& s, const float (&x)[kMlpIn]
     }
     mlp_fence_after();
     if (layer < 2) {
-      mlp_tmem_load32(t_d + warp_lane0, h);
+      // bias + ReLU, FP16, into a2 (16 columns at a time).  The next layer's MMA reads a2
+      // only after every thread's row is written (barrier at the top of the loop); a2 is
+      // free: the MMA that read it has completed.
       const float* b = layer == 0 ? s.w.b1 : s.w.b2;
 #pragma unroll
-      for (int i = 0; i < 32; ++i) h[i] = fmaxf(h[i] + b[i], 0.f);
-      // the next layer's MMA reads a2 only after every thread's rows are written (barrier
-      // at the top of the loop); a2 is free: the MMA that read it has completed
-      mlp_store_row32(s.a2, row, h);
+      for (int half = 0; half < 2; ++half) {
+        float h[16];
+        mlp_tmem_load16(t_d + warp_lane0 + half * 16, h);
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          __half2 hv[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int i = c * 8 + 2 * e;
+            hv[e] = __floats2half2_rn(fmaxf(h[i] + b[half * 16 + i], 0.f), fmaxf(h[i + 1] + b[half * 16 + i + 1], 0.f));
+          }
+          *reinterpret_cast<uint4*>(s.a2 + mlp_operand_offset(kMlpRows, row, half * 16 + c * 8)) =
+              *reinterpret_cast<uint4*>(hv);
+        }
+      }
     }
   }
   const float z = mlp_tmem_load1(t_d + warp_lane0) + s.w.b3;

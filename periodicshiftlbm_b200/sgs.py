@@ -5,6 +5,8 @@ out_scale), attached to a grid (psl_set_sgs_mlp) or evaluated alone on the tenso
 from __future__ import annotations
 
 import ctypes
+import json
+import os
 
 import numpy as np
 
@@ -152,3 +154,21 @@ def smagorinsky_nu_t(x: np.ndarray, nu: float, cs: float) -> np.ndarray:
     tau = 3.0 * nu + 0.5
     tau_les = 0.5 * tau + 0.5 * np.sqrt(tau * tau + 18.0 * cs * np.asarray(x, dtype=np.float64)[:, 7])
     return (tau_les - 0.5) / 3.0 - nu
+
+
+PACKAGED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "closure_turbulence256.json")
+
+
+def load_params(path: str = PACKAGED) -> dict:
+    """Closure parameters saved by ``save_params`` (the packaged file holds the closure
+    trained on the 512^3 -> 256^3 decaying-turbulence runs)."""
+    with open(path) as fh:
+        d = json.load(fh)
+    return {k: np.asarray(d[k], dtype=np.float64) for k in FIELDS}
+
+
+def save_params(p: dict, path: str, **meta):
+    d = {k: np.asarray(p[k], dtype=np.float64).tolist() for k in FIELDS}
+    d.update(meta)
+    with open(path, "w") as fh:
+        json.dump(d, fh)

@@ -49,7 +49,13 @@ def periodic_grid(storage="f32", n=(16, 12, 10), nu=0.01, seed=1):
     return g
 
 
-def test_constant_closure_equals_plain_update_with_added_viscosity():
+@pytest.mark.parametrize("path", ["warp", "tcgen05"])
+def test_constant_closure_equals_plain_update_with_added_viscosity(path, monkeypatch):
+    monkeypatch.setenv("PSL_CLOSURE_PATH", path)
+    _constant_closure_check()
+
+
+def _constant_closure_check():
     p = {k: np.zeros_like(v) for k, v in mo.random_params(0).items()}
     p["in_scale"] = np.ones(10)
     p["b3"] = np.float64(0.3)
@@ -68,8 +74,11 @@ def test_constant_closure_equals_plain_update_with_added_viscosity():
     b.close()
 
 
+@pytest.mark.parametrize("path", ["warp", "tcgen05"])
 @pytest.mark.parametrize("storage", ["f32", "f16"])
-def test_fused_learned_update_matches_oracle_cell_by_cell(orc, storage):
+def test_fused_learned_update_matches_oracle_cell_by_cell(orc, storage, path, monkeypatch):
+    """Both evaluations of the fused closure: per-warp MMAs (default) and CTA-wide tcgen05."""
+    monkeypatch.setenv("PSL_CLOSURE_PATH", path)
     p = mo.random_params(5)
     g = periodic_grid(storage=storage, nu=0.01)
     set_sgs_mlp(g, p, 1.0)

@@ -9,6 +9,10 @@ reports
     coefficient at the last step and averaged over the sampled last fifth of the run, and
     their relative errors against the FP64 run.
 
+A form "<storage>+mlp" runs that storage with the learned closure (the packaged weights,
+periodicshiftlbm_b200/data) in place of Smagorinsky; its errors against the FP64
+(Smagorinsky) run then hold the model difference as well as the rounding.
+
 ``python -m periodicshiftlbm_b200.precision --scale 0.5 --steps 5000`` runs the
 256x128x128 two-level subsample of the 512x256x256 Re=1e5 sphere case.
 """
@@ -55,7 +59,14 @@ def speed_error(grids, ref_grids) -> float:
 def run_form(cfg: SphereConfig, storage: str, steps: int, sample_every: int = 50):
     """Run `cfg` in one storage form; returns (grids, result dict).  The caller closes the
     grids."""
+    storage, _, closure = storage.partition("+")
     grids, case = make_sphere_grids(cfg, storage=storage)
+    if closure == "mlp":
+        from .sgs import load_params, set_sgs_mlp
+
+        params = load_params()
+        for g in grids:
+            set_sgs_mlp(g, params, g.Info.res / grids[0].Info.res)
     fine = grids[-1]
     drags = []
     t0 = time.perf_counter()
@@ -68,7 +79,7 @@ def run_form(cfg: SphereConfig, storage: str, steps: int, sample_every: int = 50
     health = [g.health() for g in grids]
     mean = float(np.mean(drags)) if drags else last
     return grids, {
-        "storage": storage,
+        "storage": storage + ("+" + closure if closure else ""),
         "steps": steps,
         "drag_last": last,
         "drag_mean_last_fifth": mean,

@@ -58,14 +58,18 @@ def softplus(z):
 
 
 def forward_device(p: dict, x: np.ndarray) -> np.ndarray:
-    """nu_t as the tensor-core path computes it (FP16 operands, FP32 accumulation)."""
+    """nu_t as the tensor-core paths compute it: normalised features x * scale + offset
+    (offset = -shift * scale, FP32), FP16 operands, the layer-1 biases as FP16 weights of a
+    constant input 1, FP32 accumulation, ReLU, FP16 activations, FP32 layer-2 biases."""
     h16 = np.float16
-    xn = ((x.astype(np.float32) - p["in_shift"].astype(np.float32)) * p["in_scale"].astype(np.float32)).astype(h16)
+    scale = p["in_scale"].astype(np.float32)
+    offset = (-p["in_shift"] * p["in_scale"]).astype(np.float32)
+    xn = (x.astype(np.float64) * scale + offset).astype(np.float32).astype(h16)
     w1 = p["w1"].astype(h16).astype(np.float32)
     w2 = p["w2"].astype(h16).astype(np.float32)
     w3 = p["w3"].astype(h16).astype(np.float32)
-    a1 = xn.astype(np.float32) @ w1.T
-    h1 = np.maximum(a1 + p["b1"].astype(np.float32), 0).astype(h16).astype(np.float32)
+    a1 = xn.astype(np.float32) @ w1.T + p["b1"].astype(h16).astype(np.float32)
+    h1 = np.maximum(a1, 0).astype(h16).astype(np.float32)
     a2 = h1 @ w2.T
     h2 = np.maximum(a2 + p["b2"].astype(np.float32), 0).astype(h16).astype(np.float32)
     z = h2 @ w3 + np.float32(p["b3"])

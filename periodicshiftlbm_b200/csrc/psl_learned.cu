@@ -37,16 +37,16 @@ void pack_warp(const psl_sgs_mlp& m, MlpWarp& d) {
   std::memset(&d, 0, sizeof(d));
   for (int o = 0; o < 32; ++o) {
     for (int k = 0; k < kMlpIn; ++k) d.w1[o * kW1Stride + k] = __float2half_rn(m.w1[o][k]);
+    d.w1[o * kW1Stride + kMlpIn] = __float2half_rn(m.b1[o]);  // times the constant input 1
     for (int k = 0; k < 32; ++k) d.w2[o * kW2Stride + k] = __float2half_rn(m.w2[o][k]);
-    d.b1[o] = m.b1[o];
     d.b2[o] = m.b2[o];
   }
   for (int k = 0; k < 32; ++k) d.w3[k] = __float2half_rn(m.w3[k]);  // row 0
   d.b3 = m.b3;
   d.out_scale = m.out_scale;
   for (int i = 0; i < kMlpIn; ++i) {
-    d.in_shift[i] = m.in_shift[i];
     d.in_scale[i] = m.in_scale[i];
+    d.in_offset[i] = -m.in_shift[i] * m.in_scale[i];
   }
 }
 
@@ -57,20 +57,18 @@ void pack(const psl_sgs_mlp& m, MlpDevice& d) {
     base[mlp_operand_offset(rows, r, k) / 2] = __float2half_rn(v);
   };
   for (int r = 0; r < kMlpHidden; ++r) {
-    for (int k = 0; k < kMlpK1; ++k) put(d.w1, kMlpHidden, r, k, k < kMlpIn ? m.w1[r][k] : 0.f);
+    for (int k = 0; k < kMlpK1; ++k)
+      put(d.w1, kMlpHidden, r, k, k < kMlpIn ? m.w1[r][k] : (k == kMlpIn ? m.b1[r] : 0.f));
     for (int k = 0; k < kMlpHidden; ++k) put(d.w2, kMlpHidden, r, k, m.w2[r][k]);
   }
   for (int r = 0; r < kMlpN3; ++r)
     for (int k = 0; k < kMlpHidden; ++k) put(d.w3, kMlpN3, r, k, r == 0 ? m.w3[k] : 0.f);
-  for (int i = 0; i < kMlpHidden; ++i) {
-    d.b1[i] = m.b1[i];
-    d.b2[i] = m.b2[i];
-  }
+  for (int i = 0; i < kMlpHidden; ++i) d.b2[i] = m.b2[i];
   d.b3 = m.b3;
   d.out_scale = m.out_scale;
   for (int i = 0; i < kMlpIn; ++i) {
-    d.in_shift[i] = m.in_shift[i];
     d.in_scale[i] = m.in_scale[i];
+    d.in_offset[i] = -m.in_shift[i] * m.in_scale[i];
   }
 }
 

@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(kMlpRows) step_learned_kernel(const __grid_con
 }
 
 template <typename S>
-__global__ void __launch_bounds__(kStepThreads) step_learned_warp_kernel(const __grid_constant__ LearnedParams<S> p) {
+__global__ void __launch_bounds__(kStepThreads, 7) step_learned_warp_kernel(const __grid_constant__ LearnedParams<S> p) {
   __shared__ MlpWarp w;
   __shared__ __align__(16) __half xtile[kStepThreads / 32][32 * kXStride];
   {

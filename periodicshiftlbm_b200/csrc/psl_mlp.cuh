@@ -47,12 +47,11 @@ struct MlpDevice {
   __half w1[kMlpHidden * kMlpK1];      // 32 x 16  (1 KB)
   __half w2[kMlpHidden * kMlpHidden];  // 32 x 32  (2 KB)
   __half w3[kMlpN3 * kMlpHidden];      // 16 x 32  (1 KB)
-  float b1[kMlpHidden];
-  float b2[kMlpHidden];
+  float b2[kMlpHidden];                // layer-1 biases ride in W1 column 10 (input 10 = 1)
   float b3;
   float out_scale;                     // nu_t = out_scale * softplus(z)
-  float in_shift[kMlpIn];              // feature normalisation: (x - shift) * scale
-  float in_scale[kMlpIn];
+  float in_scale[kMlpIn];              // feature normalisation: x * in_scale + in_offset
+  float in_offset[kMlpIn];
   float pad[2];
 };
 static_assert(sizeof(MlpDevice) % 16 == 0, "MlpDevice is copied in 16-byte units");
@@ -221,9 +220,10 @@ __device__ __forceinline__ float mlp_eval(MlpShared& s, const float (&x)[kMlpIn]
   {
     float xn[16];
 #pragma unroll
-    for (int i = 0; i < kMlpIn; ++i) xn[i] = (x[i] - s.w.in_shift[i]) * s.w.in_scale[i];
+    for (int i = 0; i < kMlpIn; ++i) xn[i] = fmaf(x[i], s.w.in_scale[i], s.w.in_offset[i]);
+    xn[kMlpIn] = 1.f;  // carries the layer-1 biases (W1 column 10)
 #pragma unroll
-    for (int i = kMlpIn; i < 16; ++i) xn[i] = 0.f;
+    for (int i = kMlpIn + 1; i < 16; ++i) xn[i] = 0.f;
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
       __half2 h[4];
@@ -270,7 +270,7 @@ __device__ __forceinline__ float mlp_eval(MlpShared& s, const float (&x)[kMlpIn]
       // bias + ReLU, FP16, into a2 (16 columns at a time).  The next layer's MMA reads a2
       // only after every thread's row is written (barrier at the top of the loop); a2 is
       // free: the MMA that read it has completed.
-      const float* b = layer == 0 ? s.w.b1 : s.w.b2;
+      const float* b = layer == 0 ? nullptr : s.w.b2;
 #pragma unroll
       for (int half = 0; half < 2; ++half) {
         float h[16];
@@ -281,7 +281,8 @@ __device__ __forceinline__ float mlp_eval(MlpShared& s, const float (&x)[kMlpIn]
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             const int i = c * 8 + 2 * e;
-            hv[e] = __floats2half2_rn(fmaxf(h[i] + b[half * 16 + i], 0.f), fmaxf(h[i + 1] + b[half * 16 + i + 1], 0.f));
+            const float bi = b ? b[half * 16 + i] : 0.f, bj = b ? b[half * 16 + i + 1] : 0.f;
+            hv[e] = __hmax2(__floats2half2_rn(h[i] + bi, h[i + 1] + bj), __float2half2_rn(0.f));
           }
           *reinterpret_cast<uint4*>(s.a2 + mlp_operand_offset(kMlpRows, row, half * 16 + c * 8)) =
               *reinterpret_cast<uint4*>(hv);

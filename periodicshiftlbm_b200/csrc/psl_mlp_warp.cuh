@@ -6,18 +6,19 @@
 // collision (its input is the second-order moments, its output the relaxation rate), so
 // every cell's whole collision state waits for it.  A CTA-wide tcgen05 MMA (psl_mlp.cuh)
 // needs three CTA barriers and three MMA round trips per 128-cell tile, during which all
-// of the CTA's warps wait; measured in the fused update kernel that ran at 5.4k MLUPS on
-// the 256^3 turbulence box against 24.1k for the same kernel with Smagorinsky.  Per warp
-// there is no barrier: each warp's 28 MMAs complete in its own instruction stream while
-// the SM's other warps keep their loads and arithmetic going.  The CTA-wide tcgen05 path
-// remains the closure's batched inference (psl_sgs_mlp_infer).
+// of the CTA's warps wait; measured in the fused update kernel on the 256^3 turbulence box
+// (FP16 storage) that ran at 10.7k MLUPS against 16.2k per warp and 25.6k with
+// Smagorinsky.  Per warp there is no barrier: each warp's 28 MMAs complete in its own
+// instruction stream while the SM's other warps keep their loads and arithmetic going.
+// The CTA-wide tcgen05 path remains the closure's batched inference (psl_sgs_mlp_infer).
 //
 // Data flow per warp:
-//   features -> normalised FP16 rows in shared memory -> ldmatrix A fragments (2 M-tiles)
-//   layer 1: 2 x 4 MMAs (K = 16); bias + ReLU + FP16 packing turns the accumulators into
-//            the A fragments of layer 2 in registers (the m16n8 accumulator layout of two
+//   features -> normalised FP16 rows in shared memory, input 10 the constant 1 that
+//   carries the layer-1 biases -> ldmatrix A fragments (2 M-tiles)
+//   layer 1: 2 x 4 MMAs (K = 16); FP16 packing + ReLU turns the accumulators into the A
+//            fragments of layer 2 in registers (the m16n8 accumulator layout of two
 //            adjacent N-tiles is the m16k16 A layout)
-//   layer 2: 2 x 4 x 2 MMAs (K = 32); same register hand-over to layer 3
+//   layer 2: 2 x 4 x 2 MMAs (K = 32); bias, packing, ReLU: the A fragments of layer 3
 //   layer 3: 2 x 2 MMAs (N = 8, row 0 of W3 holds the output weights)
 //   the output of row r sits in lane 4 (r % 8) (accumulator column 0); four shuffles bring
 //   it to lane r, the lane that owns the cell.
@@ -41,12 +42,11 @@ struct MlpWarp {
   __half w1[32 * kW1Stride];  // 1536 B
   __half w2[32 * kW2Stride];  // 2560 B
   __half w3[8 * kW2Stride];   //  640 B
-  float b1[32];
-  float b2[32];
+  float b2[32];           // layer-1 biases ride in W1 column 10 (input 10 is the constant 1)
   float b3;
   float out_scale;
-  float in_shift[kMlpIn];
-  float in_scale[kMlpIn];
+  float in_scale[kMlpIn];  // normalised feature = x * in_scale + in_offset
+  float in_offset[kMlpIn];
   float pad[2];
 };
 static_assert(sizeof(MlpWarp) % 16 == 0, "MlpWarp is copied in 16-byte units");
@@ -57,26 +57,38 @@ __device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t& r0, uint32_t& r
                : "r"(addr));
 }
 
+// d += a b (accumulate) and d = a b (fresh accumulator: C is the zero register)
 __device__ __forceinline__ void mma16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
                                          uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+  asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
       "{%0,%1,%2,%3};"
       : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
+__device__ __forceinline__ void mma16816_new(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                             uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%10,%10,%10,%10};"
+      : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1), "f"(0.f));
+}
 
+// ReLU after FP16 rounding (the same value as rounding after ReLU), two lanes at a time
 __device__ __forceinline__ uint32_t pack_relu(float a, float b) {
-  const __half2 h = __floats2half2_rn(fmaxf(a, 0.f), fmaxf(b, 0.f));
+  const __half2 h = __hmax2(__floats2half2_rn(a, b), __float2half2_rn(0.f));
   return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-// Bias + ReLU of the accumulators of N-tiles 2kk and 2kk+1 (columns 16kk..16kk+15) into
+// (bias +) ReLU of the accumulators of N-tiles 2kk and 2kk+1 (columns 16kk..16kk+15) into
 // the A fragment of K-step kk of the next layer.
+template <bool kBias>
 __device__ __forceinline__ void acc_to_a(const float (&c0)[4], const float (&c1)[4], const float* bias, int col0,
                                          uint32_t (&a)[4]) {
-  const float2 bA = *reinterpret_cast<const float2*>(bias + col0);
-  const float2 bB = *reinterpret_cast<const float2*>(bias + col0 + 8);
+  float2 bA = make_float2(0.f, 0.f), bB = make_float2(0.f, 0.f);
+  if (kBias) {
+    bA = *reinterpret_cast<const float2*>(bias + col0);
+    bB = *reinterpret_cast<const float2*>(bias + col0 + 8);
+  }
   a[0] = pack_relu(c0[0] + bA.x, c0[1] + bA.y);
   a[1] = pack_relu(c0[2] + bA.x, c0[3] + bA.y);
   a[2] = pack_relu(c1[0] + bB.x, c1[1] + bB.y);
@@ -92,9 +104,10 @@ __device__ __forceinline__ float mlp_warp_eval(const MlpWarp& w, __half* xtile, 
   {
     float xn[16];
 #pragma unroll
-    for (int i = 0; i < kMlpIn; ++i) xn[i] = (x[i] - w.in_shift[i]) * w.in_scale[i];
+    for (int i = 0; i < kMlpIn; ++i) xn[i] = fmaf(x[i], w.in_scale[i], w.in_offset[i]);
+    xn[kMlpIn] = 1.f;  // carries the layer-1 biases (W1 column 10)
 #pragma unroll
-    for (int i = kMlpIn; i < 16; ++i) xn[i] = 0.f;
+    for (int i = kMlpIn + 1; i < 16; ++i) xn[i] = 0.f;
     uint32_t p[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
@@ -123,36 +136,33 @@ __device__ __forceinline__ float mlp_warp_eval(const MlpWarp& w, __half* xtile, 
     for (int np = 0; np < 2; ++np) {
       uint32_t b[4];
       ldsm_x4(w1s + ((8 * (2 * np + (m >> 1)) + r) * kW1Stride + 8 * (m & 1)) * 2, b[0], b[1], b[2], b[3]);
-#pragma unroll
-      for (int e = 0; e < 4; ++e) c1[2 * np][e] = c1[2 * np + 1][e] = 0.f;
-      mma16816(c1[2 * np], a[0], a[1], a[2], a[3], b[0], b[1]);
-      mma16816(c1[2 * np + 1], a[0], a[1], a[2], a[3], b[2], b[3]);
+      mma16816_new(c1[2 * np], a[0], a[1], a[2], a[3], b[0], b[1]);
+      mma16816_new(c1[2 * np + 1], a[0], a[1], a[2], a[3], b[2], b[3]);
     }
     uint32_t a2[2][4];
-    acc_to_a(c1[0], c1[1], w.b1, 2 * t, a2[0]);
-    acc_to_a(c1[2], c1[3], w.b1, 16 + 2 * t, a2[1]);
+    acc_to_a<false>(c1[0], c1[1], nullptr, 0, a2[0]);
+    acc_to_a<false>(c1[2], c1[3], nullptr, 0, a2[1]);
     // ---- layer 2 ----
     float c2[4][4];
-#pragma unroll
-    for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) c2[nt][e] = 0.f;
 #pragma unroll
     for (int kk = 0; kk < 2; ++kk)
 #pragma unroll
       for (int np = 0; np < 2; ++np) {
         uint32_t b[4];
         ldsm_x4(w2s + ((8 * (2 * np + (m >> 1)) + r) * kW2Stride + 16 * kk + 8 * (m & 1)) * 2, b[0], b[1], b[2], b[3]);
-        mma16816(c2[2 * np], a2[kk][0], a2[kk][1], a2[kk][2], a2[kk][3], b[0], b[1]);
-        mma16816(c2[2 * np + 1], a2[kk][0], a2[kk][1], a2[kk][2], a2[kk][3], b[2], b[3]);
+        if (kk == 0) {
+          mma16816_new(c2[2 * np], a2[0][0], a2[0][1], a2[0][2], a2[0][3], b[0], b[1]);
+          mma16816_new(c2[2 * np + 1], a2[0][0], a2[0][1], a2[0][2], a2[0][3], b[2], b[3]);
+        } else {
+          mma16816(c2[2 * np], a2[1][0], a2[1][1], a2[1][2], a2[1][3], b[0], b[1]);
+          mma16816(c2[2 * np + 1], a2[1][0], a2[1][1], a2[1][2], a2[1][3], b[2], b[3]);
+        }
       }
     uint32_t a3[2][4];
-    acc_to_a(c2[0], c2[1], w.b2, 2 * t, a3[0]);
-    acc_to_a(c2[2], c2[3], w.b2, 16 + 2 * t, a3[1]);
+    acc_to_a<true>(c2[0], c2[1], w.b2, 2 * t, a3[0]);
+    acc_to_a<true>(c2[2], c2[3], w.b2, 16 + 2 * t, a3[1]);
     // ---- layer 3 (column 0 of the N = 8 tile) ----
-#pragma unroll
-    for (int e = 0; e < 4; ++e) z[mt][e] = 0.f;
-    mma16816(z[mt], a3[0][0], a3[0][1], a3[0][2], a3[0][3], b3[0], b3[1]);
+    mma16816_new(z[mt], a3[0][0], a3[0][1], a3[0][2], a3[0][3], b3[0], b3[1]);
     mma16816(z[mt], a3[1][0], a3[1][1], a3[1][2], a3[1][3], b3[2], b3[3]);
   }
   (void)g;

@@ -97,6 +97,17 @@ int psl_set_given(psl_grid* grid, float rho, float ux, float uy, float uz);
 int psl_set_given_field(psl_grid* grid, const float* host_rho_u);
 /* getSmagorinskyConstant (uniform per grid); 0 disables LES. */
 int psl_set_smagorinsky(psl_grid* grid, float cs);
+/* The customised update of the reference's rotating-machinery cases
+ * (M35Full/applyLocalCellUpdateCustomized.h, M40Impeller/applyLocalCellUpdateCustomized.h)
+ * on PS grids.  Selected when a body force is set or the markers hold either of:
+ *   PSL_CELL_SOLID with normal bits 1 (marker 0x0A): moving wall -- applyMovingBounceback
+ *     (boundaryConditions/applyMovingBounceback.h:8-60) with the cell's given velocity;
+ *   PSL_CELL_FLUID with normal bits 1 (marker 0x09): forced-velocity cell -- force
+ *     rho (u_given - u), the cases' getForcing hook (M35Full/m35Main.cu:101-119).
+ * Every collided cell adds the uniform body force (lattice units) and collides with the
+ * forcing collision (M40Impeller/applyCollisionCustomized.h:6-16).  Not combined with the
+ * learned closure. */
+int psl_set_body_force(psl_grid* grid, float gx, float gy, float gz);
 
 /* ---- the per-step update ---- */
 /* fillEquilibriumFromFunction (fillEquilibrium.h:1-22) with the sphere case's start hook. */

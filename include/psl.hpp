@@ -132,6 +132,16 @@ inline void setSphereCase(GridStruct& g, const psl_sphere_case& sc) {
   check(psl_apply_sphere_case(g.handle(), &sc), "setSphereCase");
 }
 // updateGrid recursion of the case driver (flowAroundSphereMainSingle.cu:158-167).
+// The customised update (moving walls, forced-velocity cells, body force): see
+// psl_set_body_force in psl.h for the marker bytes.
+inline void setBodyForce(GridStruct& g, float gx, float gy, float gz) {
+  check(psl_set_body_force(g.handle(), gx, gy, gz), "setBodyForce");
+}
+inline void getTorque(GridStruct& g, const int lo[3], const int hi[3], const float point[3], double torque[3],
+                      double force[3]) {
+  check(psl_torque(g.handle(), lo, hi, point, torque, force), "getTorque");
+}
+
 inline void updateGrid(std::vector<GridStruct>& grids, int level) {
   std::vector<psl_grid*> h(grids.size());
   for (size_t i = 0; i < grids.size(); ++i) h[i] = grids[i].handle();

@@ -20,6 +20,7 @@ from .grid import (  # noqa: F401
     getFlowReport,
     getSphereForce,
     getTorque,
+    setBodyForce,
     setGivenRhoUxUyUz,
     setSmagorinskyConstant,
     setSphereCase,

@@ -215,6 +215,13 @@ int psl_apply_sphere_case(psl_grid* g, const psl_sphere_case* sc) {
 int psl_set_markers(psl_grid* g, const uint8_t* host) {
   PSL_CHECK(g && host, PSL_ERR_INVALID, "psl_set_markers: null argument");
   DeviceGuard dg(g->device);
+  // moving walls (solid, normal bits 1) and forced-velocity cells (fluid, normal bits 1)
+  // select the customised update kernel
+  g->custom_markers = false;
+  for (uint32_t c = 0; c < g->n && !g->custom_markers; ++c) {
+    const int kind = marker_kind(host[c]);
+    g->custom_markers = (kind == kSolid || kind == kFluid) && marker_normal(host[c]) == 1;
+  }
   PSL_CUDA(cudaMemcpyAsync(g->marker, host, g->n, cudaMemcpyHostToDevice, g->stream));
   PSL_CUDA(cudaStreamSynchronize(g->stream));
   return PSL_OK;
@@ -255,6 +262,12 @@ int psl_set_given_field(psl_grid* g, const float* host) {
   }
   PSL_CUDA(cudaMemcpyAsync(g->given, host, (size_t)g->n * sizeof(float4), cudaMemcpyHostToDevice, g->stream));
   PSL_CUDA(cudaStreamSynchronize(g->stream));
+  return PSL_OK;
+}
+
+int psl_set_body_force(psl_grid* g, float gx, float gy, float gz) {
+  PSL_CHECK(g, PSL_ERR_INVALID, "psl_set_body_force: null grid");
+  g->body = make_float3(gx, gy, gz);
   return PSL_OK;
 }
 
@@ -367,7 +380,34 @@ static void launch_step(psl_grid* g) {
 int psl_apply_local_cell_update(psl_grid* g) {
   PSL_CHECK(g, PSL_ERR_INVALID, "psl_apply_local_cell_update: null grid");
   DeviceGuard dg(g->device);
-  if (g->mlp) return psl_detail_launch_learned(g);
+  const bool custom = g->custom_markers || g->body.x != 0.f || g->body.y != 0.f || g->body.z != 0.f;
+  if (g->mlp) {
+    PSL_CHECK(!custom, PSL_ERR_INVALID,
+              "psl_apply_local_cell_update: the learned closure does not combine with forcing or moving walls");
+    return psl_detail_launch_learned(g);
+  }
+  if (custom) {
+    PSL_CHECK(g->storage != kStoreF64 && 27ull * g->stride + g->n < (1ull << 32), PSL_ERR_INVALID,
+              "psl_apply_local_cell_update: forcing and moving walls need FP32/FP16/BF16 storage");
+    with_storage(g->storage, [&](auto s) {
+      using S = decltype(s);
+      if constexpr (S::kind != kStoreF64) {
+        CustomParams<S> cp;
+        cp.base.g = view<S>(g);
+        cp.base.ri = row_index<S>(g);
+        cp.base.marker = g->marker;
+        cp.base.given = g->given;
+        cp.base.given_uniform = g->given_uniform;
+        cp.base.rx = relaxation<float>(g);
+        cp.base.health = g->health;
+        cp.body = g->body;
+        step_custom_kernel<S><<<blocks_for(g->n, kStepThreads), kStepThreads, 0, g->stream>>>(cp);
+      }
+      return 0;
+    });
+    PSL_CUDA(cudaGetLastError());
+    return PSL_OK;
+  }
   with_storage(g->storage, [&](auto s) {
     launch_step<decltype(s)>(g);
     return 0;

@@ -58,8 +58,9 @@ PSL_HDI uint8_t encode_marker(int i, int j, int k, const MarkerStruct& M, const 
   if ((i > I.iSubgridStart + 1 && i < I.iSubgridEnd - 2) && (j > I.jSubgridStart + 1 && j < I.jSubgridEnd - 2) &&
       (k > I.kSubgridStart + 1 && k < I.kSubgridEnd - 2))
     return make_marker(kSkip, 0);
+  if (M.movingBounceback) return make_marker(kSolid, 1);  // moving wall (customised update)
   if (M.bounceback) return make_marker(kSolid, 0);
-  if (M.fluid) return make_marker(kFluid, 0);
+  if (M.fluid) return make_marker(kFluid, M.forcedVelocity ? 1 : 0);  // 1: forced velocity
   int nx, ny, nz;
   getOuterNormal(i, j, k, nx, ny, nz, I);
   if (M.periodicX) nx = 0;

@@ -46,6 +46,8 @@ struct psl_grid {
   int device = 0;
   bool tiled = false;               // bulk-copy tiled update kernel (N % 128 == 0)
   int batched = 0;                  // member of this many live batches (psl_batch.cu)
+  float3 body = make_float3(0.f, 0.f, 0.f);  // uniform body force (customised update)
+  bool custom_markers = false;      // moving-wall or forced-velocity markers present
   void* mlp = nullptr;              // learned closure (psl::MlpDevice), or null: Smagorinsky
   float mlp_width = 1.f;            // filter width fed to the closure
 };

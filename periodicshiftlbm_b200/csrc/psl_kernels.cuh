@@ -166,6 +166,89 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constan
 
 
 // ------------------------------------------------------------------------------------------
+// customised update: moving walls, forced-velocity cells, body force
+// ------------------------------------------------------------------------------------------
+// applyMovingBounceback (include/boundaryConditions/applyMovingBounceback.h:8-60): the
+// opposite pair (q, q+1) swaps and picks up -/+ 6 w_q (c_q . u_wall); the products are
+// rounded separately from the additions, as the reference's host build does.
+__device__ __forceinline__ void moving_bounceback(float (&f)[27], float ux, float uy, float uz) {
+#pragma unroll
+  for (int q = 1; q < 27; q += 2) {
+    const float w6 = q <= 6 ? 4.0f / 9.0f : (q <= 18 ? 1.0f / 9.0f : 1.0f / 36.0f);
+    float cu = cx(q) != 0 ? (cx(q) > 0 ? ux : -ux) : 0.f;  // c_q . u in the reference's order
+    if (cy(q) != 0) cu = cx(q) != 0 ? (cy(q) > 0 ? cu + uy : cu - uy) : (cy(q) > 0 ? uy : -uy);
+    if (cz(q) != 0) cu = (cx(q) != 0 || cy(q) != 0) ? (cz(q) > 0 ? cu + uz : cu - uz) : (cz(q) > 0 ? uz : -uz);
+    const float d = __fmul_rn(w6, cu);
+    const float t = f[q];
+    f[q] = __fadd_rn(f[q + 1], d);
+    f[q + 1] = __fsub_rn(t, d);
+  }
+}
+
+template <typename S>
+struct CustomParams {
+  StepParams<S> base;
+  float3 body;  // uniform body force on every collided cell (lattice units)
+};
+
+// The update of a customised case (the pattern of M35Full/applyLocalCellUpdateCustomized.h
+// and M40Impeller/applyLocalCellUpdateCustomized.h on PS grids):
+//   solid cell, marker normal 1    moving bounce-back with the wall velocity of the cell's
+//                                  given values (getGivenRhoUxUyUz)
+//   fluid cell, marker normal 1    forced-velocity cell: force rho (u_target - u) toward
+//                                  the given velocity (the cases' getForcing hook,
+//                                  M35Full/m35Main.cu:101-119)
+//   every collided cell            plus the uniform body force, collided with the forcing
+//                                  collision (M40Impeller/applyCollisionCustomized.h:6-16)
+template <typename S>
+__global__ void __launch_bounds__(kStepThreads) step_custom_kernel(const __grid_constant__ CustomParams<S> cp) {
+  const StepParams<S>& p = cp.base;
+  const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
+  if (cell >= p.ri.n) return;
+  const uint8_t m = p.marker[cell];
+  const int kind = marker_kind(m);
+  if (kind == kSkip) return;
+  float f[27];
+  load_cell_ri<S>(p.ri, cell, f);
+  if (kind == kSolid) {
+    if (marker_normal(m) == 1) {
+      const float4 gv = p.given ? p.given[cell] : p.given_uniform;
+      moving_bounceback(f, gv.y, gv.z, gv.w);
+    } else {
+#pragma unroll
+      for (int q = 1; q < 27; q += 2) {
+        const float t = f[q];
+        f[q] = f[q + 1];
+        f[q + 1] = t;
+      }
+    }
+  } else {
+    if (kind != kFluid) apply_boundary(m, f, p.given ? p.given[cell] : p.given_uniform);
+    float gx = cp.body.x, gy = cp.body.y, gz = cp.body.z;
+    if (kind == kFluid && marker_normal(m) == 1) {
+      float rho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+      for (int q = 0; q < 27; ++q) {
+        rho += f[q];
+        jx += cx(q) * f[q];
+        jy += cy(q) * f[q];
+        jz += cz(q) * f[q];
+      }
+      const float4 gv = p.given ? p.given[cell] : p.given_uniform;
+      gx += rho * (gv.y - jx / rho);
+      gy += rho * (gv.z - jy / rho);
+      gz += rho * (gv.w - jz / rho);
+    }
+    collide<true>(f, p.rx, gx, gy, gz);
+    if (p.health) {
+      const float r = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6];
+      if (!(r > 0.f && r < 1.0e30f)) atomicOr(p.health, 1u);
+    }
+  }
+  store_cell_ri<S>(p.ri, cell, f);
+}
+
+// ------------------------------------------------------------------------------------------
 // set-up kernels (hooks)
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ void cell_ijk(uint32_t cell, const InfoStruct& I, int& i, int& j, int& k) {

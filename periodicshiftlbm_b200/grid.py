@@ -213,6 +213,15 @@ def setGivenRhoUxUyUz(grid: GridStruct, rho, ux, uy, uz):
     call("psl_set_given", grid.handle, rho, ux, uy, uz)
 
 
+def setBodyForce(grid: GridStruct, gx: float, gy: float, gz: float):
+    """Uniform body force (lattice units) of the customised update (psl_set_body_force)."""
+    call("psl_set_body_force", grid.handle, gx, gy, gz)
+
+
+MARKER_MOVING_WALL = _lib.CELL_SOLID | (1 << 3)
+MARKER_FORCED_VELOCITY = _lib.CELL_FLUID | (1 << 3)
+
+
 def setSmagorinskyConstant(grid: GridStruct, cs: float):
     call("psl_set_smagorinsky", grid.handle, cs)
 

@@ -39,6 +39,8 @@ class CaseConfig(ctypes.Structure):
         ("wallMode", ctypes.c_int),
         ("seed", ctypes.c_uint32),
         ("noiseAmp", ctypes.c_float),
+        ("iSub2_0", ctypes.c_int), ("jSub2_0", ctypes.c_int), ("kSub2_0", ctypes.c_int),
+        ("iSub2_1", ctypes.c_int), ("jSub2_1", ctypes.c_int), ("kSub2_1", ctypes.c_int),
     ]
 
 
@@ -58,13 +60,16 @@ class SphereCase:
     seed: int = 1234
     noise: float = 1e-4
     refine: tuple | None = None  # ((i0, j0, k0), (i1, j1, k1)) coarse block, half-open
+    refine2: tuple | None = None  # a third level: block on the level-1 grid (its own cells)
 
     def to_ctypes(self) -> CaseConfig:
         c = CaseConfig()
         c.nx, c.ny, c.nz = self.nx, self.ny, self.nz
-        c.levels = 2 if self.refine else 1
+        c.levels = (3 if self.refine2 else 2) if self.refine else 1
         if self.refine:
             (c.iSub0, c.jSub0, c.kSub0), (c.iSub1, c.jSub1, c.kSub1) = self.refine
+        if self.refine2:
+            (c.iSub2_0, c.jSub2_0, c.kSub2_0), (c.iSub2_1, c.jSub2_1, c.kSub2_1) = self.refine2
         c.sphereX, c.sphereY, c.sphereZ = self.sphere
         c.sphereR = self.radius
         c.uIn = self.u_in

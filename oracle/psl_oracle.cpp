@@ -614,6 +614,10 @@ static Sim<T>* create(const CaseConfig& cfg) {
     f.oz = p.oz + p.kS * p.res - f.res * 0.5f;
     f.nx = (p.iE - p.iS) * 2; f.ny = (p.jE - p.jS) * 2; f.nz = (p.kE - p.kS) * 2;
     f.n = (long long)f.nx * f.ny * f.nz;
+    if (l + 1 < cfg.levels) {  // the next finer block lies on this grid
+      f.iS = cfg.iSub2_0; f.jS = cfg.jSub2_0; f.kS = cfg.kSub2_0;
+      f.iE = cfg.iSub2_1; f.jE = cfg.jSub2_1; f.kE = cfg.kSub2_1;
+    }
   }
   for (auto& g : sim->grids) {
     g.f.assign((size_t)27 * (size_t)g.info.n, T(0));

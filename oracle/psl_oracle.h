@@ -41,6 +41,8 @@ struct CaseConfig {
   int wallMode;  // 0 free-slip (mirror) y/z walls, 1 velocity walls
   uint32_t seed;
   float noiseAmp;
+  int iSub2_0, jSub2_0, kSub2_0;  // third level: refinement block on the level-1 grid
+  int iSub2_1, jSub2_1, kSub2_1;
 };
 
 }  // namespace oracle

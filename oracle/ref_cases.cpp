@@ -52,7 +52,7 @@ constexpr float invSqrt3 = 0.577350269f;
 // ---------------------------------------------------------------------------------------
 extern "C" struct RefCaseConfig {
   int nx, ny, nz;          // coarse grid cells
-  int levels;              // 1 or 2
+  int levels;              // 1, 2 or 3
   int iSub0, jSub0, kSub0; // refinement block on the coarse grid (cells, half-open)
   int iSub1, jSub1, kSub1;
   float sphereX, sphereY, sphereZ, sphereR;  // in coarse cell units
@@ -62,6 +62,8 @@ extern "C" struct RefCaseConfig {
   int wallMode;            // 0 = free-slip (mirror) y/z walls, 1 = velocity walls as flowAroundSphere
   uint32_t seed;
   float noiseAmp;
+  int iSub2_0, jSub2_0, kSub2_0;  // third level: refinement block on the level-1 grid
+  int iSub2_1, jSub2_1, kSub2_1;
 };
 
 static RefCaseConfig g_case;
@@ -290,6 +292,11 @@ void* ref_sim_create(const RefCaseConfig* cfg) {
     g.Info.cellCountY = (c.Info.jSubgridEnd - c.Info.jSubgridStart) * 2;
     g.Info.cellCountZ = (c.Info.kSubgridEnd - c.Info.kSubgridStart) * 2;
     g.Info.cellCount = g.Info.cellCountX * g.Info.cellCountY * g.Info.cellCountZ;
+    if (level + 1 < cfg->levels) {  // the next finer block lies on this grid
+      g.Info.iSubgridStart = cfg->iSub2_0; g.Info.iSubgridEnd = cfg->iSub2_1;
+      g.Info.jSubgridStart = cfg->jSub2_0; g.Info.jSubgridEnd = cfg->jSub2_1;
+      g.Info.kSubgridStart = cfg->kSub2_0; g.Info.kSubgridEnd = cfg->kSub2_1;
+    }
     g.fArray.setSizes(27, g.Info.cellCount);
     g.shifter = IntArrayType(27, 0);
     fillEquilibriumFromFunction(g);

@@ -32,6 +32,7 @@ class SphereConfig:
     seed: int = 1234
     noise: float = 1e-4
     refine: tuple | None = None  # ((i0, j0, k0), (i1, j1, k1)) coarse block, half-open
+    refine2: tuple | None = None  # a third level: block on the level-1 grid (its own cells)
 
     def case(self) -> SphereCase:
         return SphereCase(sphere=tuple(float(v) for v in self.sphere), radius=float(self.radius), u_in=self.u_in,
@@ -43,20 +44,28 @@ class SphereConfig:
         out = [c]
         if self.refine:
             (c.iSubgridStart, c.jSubgridStart, c.kSubgridStart), (c.iSubgridEnd, c.jSubgridEnd, c.kSubgridEnd) = self.refine
-            out.append(c.finer())
+            f = c.finer()
+            out.append(f)
+            if self.refine2:
+                (f.iSubgridStart, f.jSubgridStart, f.kSubgridStart), (f.iSubgridEnd, f.jSubgridEnd, f.kSubgridEnd) = \
+                    self.refine2
+                out.append(f.finer())
         return out
 
     def updates_per_step(self) -> int:
-        """Cells actually updated per coarse step: every non-skipped coarse cell plus two
-        fine steps of the fine interior (the fine grid's one-cell ghost layer and the coarse
-        refined interior are not updated, include/applyLocalCellUpdate.h:25-30)."""
-        n = self.nx * self.ny * self.nz
-        if not self.refine:
-            return n
-        (i0, j0, k0), (i1, j1, k1) = self.refine
-        interior = max(0, i1 - i0 - 4) * max(0, j1 - j0 - 4) * max(0, k1 - k0 - 4)
-        fx, fy, fz = 2 * (i1 - i0), 2 * (j1 - j0), 2 * (k1 - k0)
-        return n - interior + 2 * (fx - 2) * (fy - 2) * (fz - 2)
+        """Cells actually updated per coarse step: on every level the cells that are neither
+        in the fine grids' one-cell ghost layer nor in a refined interior
+        (include/applyLocalCellUpdate.h:25-30), times the level's 2^level sub-steps."""
+        total = 0
+        for level, info in enumerate(self.infos()):
+            nx, ny, nz = info.cellCountX, info.cellCountY, info.cellCountZ
+            cells = nx * ny * nz if level == 0 else (nx - 2) * (ny - 2) * (nz - 2)
+            if info.iSubgridEnd > info.iSubgridStart:
+                cells -= (max(0, info.iSubgridEnd - info.iSubgridStart - 4) *
+                          max(0, info.jSubgridEnd - info.jSubgridStart - 4) *
+                          max(0, info.kSubgridEnd - info.kSubgridStart - 4))
+            total += cells * 2 ** level
+        return total
 
     def reference_updates_per_step(self) -> int:
         """The reference driver's own count (flowAroundSphereMainSingle.cu:225-234), which

@@ -10,7 +10,8 @@ def config_from_case(case) -> SphereConfig:
     """oracle.bindings.SphereCase -> the package's SphereConfig (same fields)."""
     return SphereConfig(name="test", nx=case.nx, ny=case.ny, nz=case.nz, sphere=tuple(case.sphere),
                         radius=case.radius, u_in=case.u_in, nu=case.nu, smagorinsky=case.smagorinsky,
-                        wall_mode=case.wall_mode, seed=case.seed, noise=case.noise, refine=case.refine)
+                        wall_mode=case.wall_mode, seed=case.seed, noise=case.noise, refine=case.refine,
+                        refine2=case.refine2)
 
 
 class GpuSim:

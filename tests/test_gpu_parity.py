@@ -134,3 +134,20 @@ def test_config1_1000_steps_matches_reference(ref):
     assert l2 < 1e-6
     assert max_rel < 1e-5
     sim.close()
+
+
+def test_three_levels_match_reference(ref):
+    """Three refinement levels through psl_update_grid's recursion against the reference's
+    own code: shifts exact, populations of every level within FP32 rounding."""
+    c = SphereCase(nx=32, ny=24, nz=24, sphere=(13.0, 12.0, 12.0), radius=2.5, nu=0.004, smagorinsky=0.1,
+                   refine=((6, 6, 6), (22, 18, 18)), refine2=((8, 6, 6), (24, 18, 18)))
+    g = GpuSim(c)
+    r = ref.sim(c)
+    assert g.levels == 3
+    g.run(10)
+    r.run(10)
+    for lev in range(3):
+        assert np.array_equal(g.shifts(lev), r.shifts(lev)), lev
+        assert rel(g.populations(lev), r.populations(lev)) < 1e-5, lev
+    assert abs(g.drag() - r.drag()) <= 1e-4 * abs(r.drag())
+    g.close()

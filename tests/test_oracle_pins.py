@@ -141,3 +141,21 @@ def test_live_reference_random_states(ref, orc):
             uu = rng.uniform(-0.05, 0.05, 3)
             assert np.max(np.abs(orc.mbbc(nrm, 1.0, *uu, f) - ref.mbbc(nrm, 1.0, *uu, f))) < 2e-7
             assert np.array_equal(orc.mirror(nrm, f), ref.mirror(nrm, f))
+
+
+THREE_LEVELS = SphereCase(nx=32, ny=24, nz=24, sphere=(13.0, 12.0, 12.0), radius=2.5, nu=0.004, smagorinsky=0.1,
+                          refine=((6, 6, 6), (22, 18, 18)), refine2=((8, 6, 6), (24, 18, 18)))
+
+
+def test_three_levels_oracle_matches_reference(ref, orc):
+    """The updateGrid recursion over three levels (flowAroundSphereMainSingle.cu:158-167):
+    the restatement against the reference's own code, every level."""
+    a = ref.sim(THREE_LEVELS)
+    b = orc.sim(THREE_LEVELS)
+    a.run(6)
+    b.run(6)
+    for lev in range(3):
+        assert np.array_equal(a.shifts(lev), b.shifts(lev)), lev
+        fa, fb = a.populations(lev), b.populations(lev)
+        assert np.max(np.abs(fa - fb) / np.abs(fa)) < 1e-5, lev
+    assert abs(a.drag() - b.drag()) <= 1e-4 * abs(a.drag())

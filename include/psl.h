@@ -158,6 +158,17 @@ typedef struct psl_flow_report {
 int psl_get_flow_report(psl_grid* const* grids, int levels, int plane, int cut_index, const float* bounds6,
                         psl_flow_report* report);
 
+/* exportSectionCutPlotGeneral (plotter/exportSectionCutPlot.h:1-88) without the file: the
+ * section `plane` at layer `cut` of one grid, V x H pixels (XY: H = Nx, V = Ny; ZY: H = Nz,
+ * V = Ny; ZX: H = Nz, V = Nx), each five floats (p, u_horizontal, u_vertical, u_normal,
+ * solid) in physical units: p = (rho - 1) rho_nominal_phys soundspeed_phys^2 and
+ * u (res / 1000) / dt_phys, rho and u summed in FP32 in getRhoUxUyUz's order
+ * (cellFunctions.h:135-155).  Writes V and H; with out == NULL only those.  out holds
+ * `capacity` floats on the host (at least 5 V H).  The reference's plotter file is this
+ * record behind the header {plot number, V, H, 5} (int32). */
+int psl_export_section_cut(psl_grid* grid, int plane, int cut, float rho_nominal_phys, float soundspeed_phys,
+                           float* out, long long capacity, int* vertical, int* horizontal);
+
 /* Momentum-exchange force over the solid cells of the box [box_lo3, box_hi3), FP64, on
  * caller-owned buffers, allocating no device memory.  No counterpart in the reference.
  * For callers that cannot call cudaMalloc when they need the force: step loops running

@@ -15,6 +15,9 @@ from .grid import (  # noqa: F401
     applyStreaming,
     debug_cells,
     drag_coefficient,
+    exportHistoryData,
+    exportSectionCutPlot,
+    sectionCut,
     fillEquilibriumFromFunction,
     getSphereDrag,
     getFlowReport,

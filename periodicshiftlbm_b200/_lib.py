@@ -130,6 +130,9 @@ _SIGNATURES = {
     "psl_get_flow_report": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_void_p, ctypes.POINTER(PslFlowReport)]),
     "psl_set_body_force": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float]),
+    "psl_export_section_cut": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                              ctypes.c_float, ctypes.c_void_p, ctypes.c_longlong,
+                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "psl_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "psl_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "psl_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

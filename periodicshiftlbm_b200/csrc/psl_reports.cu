@@ -1,5 +1,6 @@
-// FP64 reductions for flow reports (include/psl.h): torque of the momentum exchange on
-// solid cells, and the plane flow report composed over refinement levels.
+// Flow reports (include/psl.h): torque of the momentum exchange on solid cells and the
+// plane flow report composed over refinement levels (FP64 reductions), and the section-cut
+// export of the reference's plotters.
 //
 // psl_get_flow_report follows getFlowReportGeneral (include/flowReportFunctions.h:2-251): the
 // physical bounds are mapped to index bounds on the finest grid; the finest level whose
@@ -195,7 +196,108 @@ __global__ void __launch_bounds__(kRedThreads) section_sum_kernel(Section sec, d
   block_sum_store<5>(acc, partial);
 }
 
+// getRhoUxUyUz (cellFunctions.h:135-155) in FP32 with the reference's order of additions.
+__device__ __forceinline__ void rho_u_reference_order(const float (&f)[27], float& rho, float& ux, float& uy, float& uz) {
+  float r = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+  for (int q = 0; q < 27; ++q) {
+    r = __fadd_rn(r, f[q]);
+    if (cx(q) != 0) jx = cx(q) > 0 ? __fadd_rn(jx, f[q]) : __fsub_rn(jx, f[q]);
+    if (cy(q) != 0) jy = cy(q) > 0 ? __fadd_rn(jy, f[q]) : __fsub_rn(jy, f[q]);
+    if (cz(q) != 0) jz = cz(q) > 0 ? __fadd_rn(jz, f[q]) : __fsub_rn(jz, f[q]);
+  }
+  rho = r;
+  ux = __fdiv_rn(jx, r);
+  uy = __fdiv_rn(jy, r);
+  uz = __fdiv_rn(jz, r);
+}
+
+// One pixel of exportSectionCutPlotGeneral (include/plotter/exportSectionCutPlot.h:1-88):
+// (p, u_horizontal, u_vertical, u_normal, solid) in physical units.
+template <typename S>
+__global__ void section_export_kernel(GridView<S> g, const uint8_t* marker, int nx, int ny, int plane, int cut,
+                                      int horizontal, int vertical, float vel_scale, float dt, float p_scale,
+                                      float* out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= horizontal * vertical) return;
+  const int h = t % horizontal, v = t / horizontal;
+  int i, j, k;
+  if (plane == PSL_PLANE_XY) {
+    i = h; j = v; k = cut;
+  } else if (plane == PSL_PLANE_ZY) {
+    i = cut; j = v; k = h;
+  } else {
+    i = v; j = cut; k = h;
+  }
+  const uint32_t cell = ((uint32_t)k * ny + j) * nx + i;
+  float f[27];
+#pragma unroll
+  for (int q = 0; q < 27; ++q) f[q] = (float)S::load_q(g.fq[q] + shifted(cell, g.shift[q], g.n), q);
+  float rho, ux, uy, uz;
+  rho_u_reference_order(f, rho, ux, uy, uz);
+  // convertToPhysicalVelocity / convertToPhysicalPressure (cellFunctions.h:200-219)
+  ux = __fdiv_rn(__fmul_rn(ux, vel_scale), dt);
+  uy = __fdiv_rn(__fmul_rn(uy, vel_scale), dt);
+  uz = __fdiv_rn(__fmul_rn(uz, vel_scale), dt);
+  const float p = __fmul_rn(__fsub_rn(rho, 1.f), p_scale);
+  float uh, uv, un;
+  if (plane == PSL_PLANE_XY) {
+    uh = ux; uv = uy; un = uz;
+  } else if (plane == PSL_PLANE_ZY) {
+    uh = uz; uv = uy; un = ux;
+  } else {
+    uh = uz; uv = ux; un = uy;
+  }
+  float* o = out + ((size_t)v * horizontal + h) * 5;
+  o[0] = p;
+  o[1] = uh;
+  o[2] = uv;
+  o[3] = un;
+  o[4] = marker_kind(marker[cell]) == kSolid ? 1.f : 0.f;
+}
+
 }  // namespace
+
+int psl_export_section_cut(psl_grid* g, int plane, int cut, float rho_nominal_phys, float soundspeed_phys,
+                           float* out, long long capacity, int* vertical, int* horizontal) {
+  if (!g || !vertical || !horizontal || plane < PSL_PLANE_XY || plane > PSL_PLANE_ZX)
+    return fail(PSL_ERR_INVALID, "psl_export_section_cut: bad argument");
+  const psl_info& I = g->info;
+  int H, V, depth;
+  if (plane == PSL_PLANE_XY) {
+    H = I.cell_count_x; V = I.cell_count_y; depth = I.cell_count_z;
+  } else if (plane == PSL_PLANE_ZY) {
+    H = I.cell_count_z; V = I.cell_count_y; depth = I.cell_count_x;
+  } else {
+    H = I.cell_count_z; V = I.cell_count_x; depth = I.cell_count_y;
+  }
+  *vertical = V;
+  *horizontal = H;
+  if (!out) return PSL_OK;  // size query
+  if (cut < 0 || cut >= depth) return fail(PSL_ERR_INVALID, "psl_export_section_cut: cut index outside the grid");
+  const size_t count = (size_t)V * H * 5;
+  if (capacity < (long long)count) return fail(PSL_ERR_INVALID, "psl_export_section_cut: output buffer too small");
+  DeviceGuard dg(g->device);
+  float* dev = nullptr;
+  REP_CUDA(cudaMalloc(&dev, count * sizeof(float)));
+  // convertToPhysicalVelocity: u (res / 1000) / dtPhys; convertToPhysicalPressure:
+  // (rho - 1) rhoNominalPhys soundspeedPhys^2
+  const float vel_scale = I.res / 1000.f;
+  const float p_scale = rho_nominal_phys * soundspeed_phys * soundspeed_phys;
+  with_storage(g->storage, [&](auto s) {
+    using S = decltype(s);
+    section_export_kernel<S><<<(H * V + 255) / 256, 256, 0, g->stream>>>(view_of<S>(g), g->marker, I.cell_count_x,
+                                                                        I.cell_count_y, plane, cut, H, V, vel_scale,
+                                                                        I.dt_phys, p_scale, dev);
+    return 0;
+  });
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, dev, count * sizeof(float), cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  cudaFree(dev);
+  if (e != cudaSuccess) return fail(PSL_ERR_CUDA, std::string("psl_export_section_cut: ") + cudaGetErrorString(e));
+  return PSL_OK;
+}
 
 int psl_torque(psl_grid* g, const int* lo3, const int* hi3, const float* point3, double* torque3, double* force3) {
   if (!g || !lo3 || !hi3 || !point3 || !torque3) return fail(PSL_ERR_INVALID, "psl_torque: null argument");

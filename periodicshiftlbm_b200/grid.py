@@ -306,6 +306,47 @@ def getFlowReport(grids, plane: str, cut_index: int, bounds) -> dict:
     return {"ux": r.ux, "uy": r.uy, "uz": r.uz, "rho": r.rho, "area": r.area}
 
 
+def sectionCut(grid: GridStruct, plane: str, cut_index: int, rho_nominal_phys: float = 1000.0,
+               soundspeed_phys: float = 1.0) -> np.ndarray:
+    """The section of exportSectionCutPlotGeneral (plotter/exportSectionCutPlot.h:1-88) as a
+    [vertical, horizontal, 5] float32 array: p, u_horizontal, u_vertical, u_normal, solid."""
+    v, h = ctypes.c_int(), ctypes.c_int()
+    call("psl_export_section_cut", grid.handle, PLANES[plane], int(cut_index), rho_nominal_phys, soundspeed_phys,
+         None, 0, ctypes.byref(v), ctypes.byref(h))
+    out = np.empty((v.value, h.value, 5), dtype=np.float32)
+    call("psl_export_section_cut", grid.handle, PLANES[plane], int(cut_index), rho_nominal_phys, soundspeed_phys,
+         out.ctypes.data, out.size, ctypes.byref(v), ctypes.byref(h))
+    return out
+
+
+def write_section_cut(path: str, plot_number: int, section: np.ndarray):
+    """The file the reference's plotters read (exportSectionCutPlot.h:64-88, plotter.py):
+    int32 {plot number, vertical, horizontal, 5}, then the float32 records row by row."""
+    section = np.ascontiguousarray(section, dtype=np.float32)
+    with open(path, "wb") as fh:
+        np.array([plot_number, section.shape[0], section.shape[1], section.shape[2]], dtype=np.int32).tofile(fh)
+        section.tofile(fh)
+
+
+def exportSectionCutPlot(grid: GridStruct, plane: str, cut_index: int, plot_number: int,
+                         path: str = "/dev/shm/sim_data.bin", rho_nominal_phys: float = 1000.0,
+                         soundspeed_phys: float = 1.0) -> np.ndarray:
+    """exportSectionCutPlotXY/ZY/ZX: the section written where the reference's plotter
+    looks for it; returns the section."""
+    sec = sectionCut(grid, plane, cut_index, rho_nominal_phys, soundspeed_phys)
+    write_section_cut(path, plot_number, sec)
+    return sec
+
+
+def exportHistoryData(history, current_iteration: int, path: str = "/dev/shm/historyData.bin"):
+    """exportHistoryData (exportSectionCutPlot.h:994-1001): int32 count = iteration + 1,
+    then that many float32 history values."""
+    count = int(current_iteration) + 1
+    with open(path, "wb") as fh:
+        np.array([count], dtype=np.int32).tofile(fh)
+        np.asarray(history, dtype=np.float32)[:count].tofile(fh)
+
+
 def drag_coefficient(drag_lattice: float, grid_info: InfoStruct, case: SphereCase, coarse_res: float = 1.0) -> float:
     """Cd = F / (rho U^2 pi D^2 / 8) with F and U in the units of the grid the force was
     summed on (the reference converts both to physical units: the factors cancel)."""

@@ -109,6 +109,23 @@ int psl_set_smagorinsky(psl_grid* grid, float cs);
  * learned closure. */
 int psl_set_body_force(psl_grid* grid, float gx, float gy, float gz);
 
+/* Scalar transport (scalarTransportFunctions.h:10-176, Zhang, Fan & Chen 2011): 27 FP32
+ * scalar populations T_q stored and streamed like the flow populations; in
+ * psl_apply_local_cell_update they bounce back and mirror with f, take the prescribed
+ * concentration where one is given, and collide after the flow collision with relaxation
+ * time tauT (applyScalarTransportCollision).  Single grids (the coarse/fine transfer does
+ * not carry T); not combined with forcing, moving walls or the learned closure.  T starts
+ * at 0. */
+int psl_enable_scalar_transport(psl_grid* grid, float tauT);
+/* Per-cell prescribed concentration, N host floats, NaN where none (getGivenT with the
+ * givenT marker); NULL removes it. */
+int psl_set_scalar_given_field(psl_grid* grid, const float* givenT);
+/* Scalar populations in logical order [27][N] (host). */
+int psl_get_scalar_populations(psl_grid* grid, float* host);
+int psl_set_scalar_populations(psl_grid* grid, const float* host);
+/* Concentration of every cell, sum_q f_q T_q / rho (FP64), N host doubles. */
+int psl_get_scalar(psl_grid* grid, double* host);
+
 /* ---- the per-step update ---- */
 /* fillEquilibriumFromFunction (fillEquilibrium.h:1-22) with the sphere case's start hook. */
 int psl_fill_equilibrium_sphere(psl_grid* grid, const psl_sphere_case* sc);

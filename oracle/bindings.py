@@ -183,6 +183,10 @@ class RefLib(_SimLib):
         L.ref_mirror.argtypes = [i, i, i, vp]
         L.ref_bounceback.argtypes = [vp]
         L.ref_moving_bounceback.argtypes = [vp, f, f, f]
+        L.ref_scalar_collision.argtypes = [vp, vp, f]
+        L.ref_sim_enable_scalar.argtypes = [vp, f, ctypes.c_int]
+        L.ref_sim_set_T.argtypes = [vp, vp]
+        L.ref_sim_get_T.argtypes = [vp, vp]
         L.ref_rescale.argtypes = [vp, i]
         L.ref_streaming.argtypes = [i, i, i, vp]
         for n in ("ref_sim_periodic_x", "ref_sim_periodic_y", "ref_sim_streaming"):
@@ -254,6 +258,27 @@ class RefLib(_SimLib):
         a = np.array(f, dtype=np.float32)
         self.lib.ref_moving_bounceback(a.ctypes.data, ux, uy, uz)
         return a
+
+    def scalar_collision(self, f, T, tauT):
+        a = np.array(f, dtype=np.float32)
+        t = np.array(T, dtype=np.float32)
+        self.lib.ref_scalar_collision(a.ctypes.data, t.ctypes.data, tauT)
+        return t
+
+    def enable_scalar(self, sim, tauT: float, inlet: bool):
+        """The reference's scalar-transport update on grid 0 of `sim` (T starts at 0); with
+        `inlet`, concentration 1 is prescribed on the lower half (j < Ny/2) of the inlet
+        plane and 0 on the upper half."""
+        self.lib.ref_sim_enable_scalar(sim.h, tauT, 1 if inlet else 0)
+
+    def scalar_populations(self, sim):
+        out = np.empty((27, sim.cell_count(0)), dtype=np.float32)
+        self.lib.ref_sim_get_T(sim.h, out.ctypes.data)
+        return out
+
+    def set_scalar_populations(self, sim, t):
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        self.lib.ref_sim_set_T(sim.h, t.ctypes.data)
 
     def rescale(self, f, coarse_to_fine: bool):
         a = np.array(f, dtype=np.float32)

@@ -141,6 +141,27 @@ __cuda_callable__ void getGivenRhoUxUyUz(const int& iCell, const int& jCell, con
 }
 
 #include "include/applyLocalCellUpdate.h"
+
+// Scalar transport (include/scalarTransportFunctions.h): the case hooks it calls -- a given
+// concentration on the inlet plane, T = 1 on its lower half (j < Ny/2), 0 above -- and
+// declarations of the two functions its update calls before the header defines them.
+static bool g_scalar_inlet = false;
+__cuda_callable__ void getScalarTransportMarkers(const int& iCell, const int& jCell, const int& kCell,
+                                                 ScalarTransportMarkerStruct& M, const InfoStruct& Info) {
+  if (g_scalar_inlet && iCell == 0) M.givenT = 1;
+}
+__cuda_callable__ void getGivenT(const int& iCell, const int& jCell, const int& kCell, float& T, const InfoStruct& Info) {
+  T = (jCell < Info.cellCountY / 2) ? 1.f : 0.f;
+}
+__host__ __device__ void applyScalarTransportCollision(float (&f)[27], float (&T)[27], const float& tauT);
+__host__ __device__ void applyScalarTransportGivenT(float (&T)[27], float& givenT);
+// The header's update tests a MarkerStruct member `mirror` that include/types.h does not
+// declare; for this build it reads the periodicZ flag instead, which the sphere hooks never
+// set, so scalar runs use the velocity-wall sphere case (wallMode 1) and no mirror cells.
+#define mirror periodicZ
+#include "include/scalarTransportFunctions.h"
+#undef mirror
+
 #include "include/fillEquilibrium.h"
 #include "include/gridRefinementFunctions.h"
 #include "include/boundaryConditions/periodicXY.h"
@@ -241,10 +262,17 @@ static double sphereDragLattice(GridStruct& Grid) {
 struct RefSim {
   std::vector<GridStruct> grids;
   bool freeSlip = false;
+  bool scalar = false;                 // single-level scalar transport run
+  ScalarTransportStruct transport;     // T populations of grid 0
 };
 
 static void updateLevel(RefSim& sim, int level) {
   std::vector<GridStruct>& grids = sim.grids;
+  if (sim.scalar) {  // the reference's scalar-transport update (scalarTransportFunctions.h:10-107)
+    applyStreaming(grids[0]);
+    applyLocalCellUpdate(grids[0], sim.transport);
+    return;
+  }
   applyStreaming(grids[level]);
   if (sim.freeSlip) applyLocalCellUpdateFreeSlip(grids[level]);
   else applyLocalCellUpdate(grids[level]);
@@ -395,6 +423,50 @@ void ref_restore_rho_u(int nx, int ny, int nz, const float* f, float* out4) {
 }
 void ref_mirror(int nx, int ny, int nz, float* f) { applyMirror(nx, ny, nz, *reinterpret_cast<float (*)[27]>(f)); }
 void ref_bounceback(float* f) { applyBounceback(*reinterpret_cast<float (*)[27]>(f)); }
+void ref_scalar_collision(float* f, float* T, float tauT) {
+  applyScalarTransportCollision(*reinterpret_cast<float (*)[27]>(f), *reinterpret_cast<float (*)[27]>(T), tauT);
+}
+
+// Scalar transport on grid 0 (single-level runs): T populations in logical order [27][N],
+// stored at the same shifted addresses as f.
+void ref_sim_enable_scalar(void* h, float tauT, int inlet) {
+  RefSim* sim = static_cast<RefSim*>(h);
+  GridStruct& g = sim->grids[0];
+  sim->scalar = true;
+  g_scalar_inlet = inlet != 0;
+  sim->transport.tauT = tauT;
+  sim->transport.TArray.setSizes(27, g.Info.cellCount);
+  sim->transport.TArray.setValue(0.f);
+}
+void ref_sim_set_T(void* h, const float* in) {
+  RefSim* sim = static_cast<RefSim*>(h);
+  GridStruct& g = sim->grids[0];
+  const long long N = g.Info.cellCount;
+  auto v = sim->transport.TArray.getView();
+  for (int q = 0; q < 27; ++q) {
+    const long long s = g.shifter[q];
+    for (long long c = 0; c < N; ++c) {
+      long long a = c + s;
+      if (a >= N) a -= N;
+      v(q, a) = in[(size_t)q * N + c];
+    }
+  }
+}
+void ref_sim_get_T(void* h, float* out) {
+  RefSim* sim = static_cast<RefSim*>(h);
+  GridStruct& g = sim->grids[0];
+  const long long N = g.Info.cellCount;
+  auto v = sim->transport.TArray.getConstView();
+  for (int q = 0; q < 27; ++q) {
+    const long long s = g.shifter[q];
+    for (long long c = 0; c < N; ++c) {
+      long long a = c + s;
+      if (a >= N) a -= N;
+      out[(size_t)q * N + c] = v(q, a);
+    }
+  }
+}
+
 void ref_moving_bounceback(float* f, float ux, float uy, float uz) {
   applyMovingBounceback(*reinterpret_cast<float (*)[27]>(f), ux, uy, uz);
 }

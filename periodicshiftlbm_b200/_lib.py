@@ -133,6 +133,11 @@ _SIGNATURES = {
     "psl_export_section_cut": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                               ctypes.c_float, ctypes.c_void_p, ctypes.c_longlong,
                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "psl_enable_scalar_transport": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_float]),
+    "psl_set_scalar_given_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "psl_get_scalar_populations": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "psl_set_scalar_populations": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "psl_get_scalar": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "psl_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "psl_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

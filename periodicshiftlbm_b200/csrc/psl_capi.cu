@@ -182,6 +182,8 @@ int psl_grid_destroy(psl_grid* g) {
   if (g->health) cudaFree(g->health);
   if (g->scratch) cudaFree(g->scratch);
   if (g->mlp) cudaFree(g->mlp);
+  if (g->T) cudaFree(g->T);
+  if (g->givenT) cudaFree(g->givenT);
   delete g;
   return PSL_OK;
 }
@@ -268,6 +270,109 @@ int psl_set_given_field(psl_grid* g, const float* host) {
 int psl_set_body_force(psl_grid* g, float gx, float gy, float gz) {
   PSL_CHECK(g, PSL_ERR_INVALID, "psl_set_body_force: null grid");
   g->body = make_float3(gx, gy, gz);
+  return PSL_OK;
+}
+
+// ---- scalar transport ----
+static GridView<StoreF32> scalar_view(const psl_grid* g) {
+  GridView<StoreF32> v;
+  for (int q = 0; q < 27; ++q) {
+    v.fq[q] = g->T + (size_t)q * g->stride;
+    v.shift[q] = g->shift[q];
+  }
+  v.n = g->n;
+  return v;
+}
+
+int psl_enable_scalar_transport(psl_grid* g, float tauT) {
+  PSL_CHECK(g, PSL_ERR_INVALID, "psl_enable_scalar_transport: null grid");
+  PSL_CHECK(tauT > 0.5f, PSL_ERR_INVALID, "psl_enable_scalar_transport: tau_T must exceed 1/2");
+  DeviceGuard dg(g->device);
+  if (!g->T) {
+    const size_t bytes = 27 * g->stride * sizeof(float);
+    cudaError_t e = cudaMalloc(&g->T, bytes);
+    if (e == cudaSuccess) e = cudaMemsetAsync(g->T, 0, bytes, g->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+    if (e != cudaSuccess) {
+      if (g->T) cudaFree(g->T);
+      g->T = nullptr;
+      cudaGetLastError();
+      return fail(PSL_ERR_NOMEM, std::string("psl_enable_scalar_transport: ") + cudaGetErrorString(e));
+    }
+  }
+  g->tauT = tauT;
+  return PSL_OK;
+}
+
+int psl_set_scalar_given_field(psl_grid* g, const float* host) {
+  PSL_CHECK(g, PSL_ERR_INVALID, "psl_set_scalar_given_field: null grid");
+  DeviceGuard dg(g->device);
+  if (!host) {
+    if (g->givenT) {
+      PSL_CUDA(cudaStreamSynchronize(g->stream));
+      cudaFree(g->givenT);
+      g->givenT = nullptr;
+    }
+    return PSL_OK;
+  }
+  if (!g->givenT) PSL_CUDA(cudaMalloc(&g->givenT, (size_t)g->n * sizeof(float)));
+  PSL_CUDA(cudaMemcpyAsync(g->givenT, host, (size_t)g->n * sizeof(float), cudaMemcpyHostToDevice, g->stream));
+  PSL_CUDA(cudaStreamSynchronize(g->stream));
+  return PSL_OK;
+}
+
+static int scalar_rows(psl_grid* g, float* host, bool get) {
+  float* tmp = nullptr;
+  PSL_CUDA(cudaMalloc(&tmp, (size_t)g->n * sizeof(float)));
+  cudaError_t e = cudaStreamSynchronize(g->stream);
+  const GridView<StoreF32> v = scalar_view(g);
+  for (int q = 0; q < 27 && e == cudaSuccess; ++q) {
+    if (get) {
+      gather_logical_kernel<StoreF32><<<blocks_for(g->n, 256), 256, 0, g->stream>>>(v, q, tmp);
+      e = cudaGetLastError();
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(host + (size_t)q * g->n, tmp, (size_t)g->n * sizeof(float), cudaMemcpyDeviceToHost, g->stream);
+    } else {
+      e = cudaMemcpyAsync(tmp, host + (size_t)q * g->n, (size_t)g->n * sizeof(float), cudaMemcpyHostToDevice, g->stream);
+      if (e == cudaSuccess) {
+        scatter_logical_kernel<StoreF32><<<blocks_for(g->n, 256), 256, 0, g->stream>>>(v, q, tmp);
+        e = cudaGetLastError();
+      }
+    }
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return fail(PSL_ERR_CUDA, std::string("psl scalar populations: ") + cudaGetErrorString(e));
+  return PSL_OK;
+}
+
+int psl_get_scalar_populations(psl_grid* g, float* host) {
+  PSL_CHECK(g && host && g->T, PSL_ERR_INVALID, "psl_get_scalar_populations: no scalar transport on this grid");
+  DeviceGuard dg(g->device);
+  return scalar_rows(g, host, true);
+}
+
+int psl_set_scalar_populations(psl_grid* g, const float* host) {
+  PSL_CHECK(g && host && g->T, PSL_ERR_INVALID, "psl_set_scalar_populations: no scalar transport on this grid");
+  DeviceGuard dg(g->device);
+  return scalar_rows(g, const_cast<float*>(host), false);
+}
+
+int psl_get_scalar(psl_grid* g, double* host) {
+  PSL_CHECK(g && host && g->T, PSL_ERR_INVALID, "psl_get_scalar: no scalar transport on this grid");
+  DeviceGuard dg(g->device);
+  double* tmp = nullptr;
+  PSL_CUDA(cudaMalloc(&tmp, (size_t)g->n * sizeof(double)));
+  with_storage(g->storage, [&](auto s) {
+    using S = decltype(s);
+    scalar_mean_kernel<S><<<blocks_for(g->n, 256), 256, 0, g->stream>>>(view<S>(g), scalar_view(g), tmp);
+    return 0;
+  });
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, (size_t)g->n * sizeof(double), cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return fail(PSL_ERR_CUDA, std::string("psl_get_scalar: ") + cudaGetErrorString(e));
   return PSL_OK;
 }
 
@@ -381,6 +486,38 @@ int psl_apply_local_cell_update(psl_grid* g) {
   PSL_CHECK(g, PSL_ERR_INVALID, "psl_apply_local_cell_update: null grid");
   DeviceGuard dg(g->device);
   const bool custom = g->custom_markers || g->body.x != 0.f || g->body.y != 0.f || g->body.z != 0.f;
+  if (g->T) {
+    PSL_CHECK(!custom && !g->mlp, PSL_ERR_INVALID,
+              "psl_apply_local_cell_update: scalar transport does not combine with forcing, moving walls or the "
+              "learned closure");
+    PSL_CHECK(g->storage != kStoreF64 && 27ull * g->stride + g->n < (1ull << 32), PSL_ERR_INVALID,
+              "psl_apply_local_cell_update: scalar transport needs FP32/FP16/BF16 storage");
+    with_storage(g->storage, [&](auto s) {
+      using S = decltype(s);
+      if constexpr (S::kind != kStoreF64) {
+        ScalarParams<S> sp;
+        sp.base.g = view<S>(g);
+        sp.base.ri = row_index<S>(g);
+        sp.base.marker = g->marker;
+        sp.base.given = g->given;
+        sp.base.given_uniform = g->given_uniform;
+        sp.base.rx = relaxation<float>(g);
+        sp.base.health = g->health;
+        sp.T.base = g->T;
+        sp.T.n = g->n;
+        for (int q = 0; q < 27; ++q) {
+          sp.T.off[q] = sp.base.ri.off[q];
+          sp.T.lim[q] = sp.base.ri.lim[q];
+        }
+        sp.givenT = g->givenT;
+        sp.tauT = g->tauT;
+        step_scalar_kernel<S><<<blocks_for(g->n, kStepThreads), kStepThreads, 0, g->stream>>>(sp);
+      }
+      return 0;
+    });
+    PSL_CUDA(cudaGetLastError());
+    return PSL_OK;
+  }
   if (g->mlp) {
     PSL_CHECK(!custom, PSL_ERR_INVALID,
               "psl_apply_local_cell_update: the learned closure does not combine with forcing or moving walls");

@@ -48,6 +48,9 @@ struct psl_grid {
   int batched = 0;                  // member of this many live batches (psl_batch.cu)
   float3 body = make_float3(0.f, 0.f, 0.f);  // uniform body force (customised update)
   bool custom_markers = false;      // moving-wall or forced-velocity markers present
+  float* T = nullptr;               // scalar-transport populations (27 FP32 rows), or null
+  float* givenT = nullptr;          // per-cell prescribed concentration (NaN: none), or null
+  float tauT = 1.f;
   void* mlp = nullptr;              // learned closure (psl::MlpDevice), or null: Smagorinsky
   float mlp_width = 1.f;            // filter width fed to the closure
 };

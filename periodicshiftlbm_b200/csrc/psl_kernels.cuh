@@ -249,6 +249,109 @@ __global__ void __launch_bounds__(kStepThreads) step_custom_kernel(const __grid_
 }
 
 // ------------------------------------------------------------------------------------------
+// scalar transport (include/scalarTransportFunctions.h:10-176)
+// ------------------------------------------------------------------------------------------
+// Collision of the scalar populations T_q after the flow collision, after Zhang, Fan & Chen
+// (2011, eqs 2.5-2.7) as applyScalarTransportCollision uses them: with the post-collision
+// populations f, T_mean = sum f T / rho, S = sum c (f (T - T_mean)),
+// F_q = 3/rho (c_q - u) . S and T_q <- T_mean + (1 - 1/tau_T) F_q.  sum f T is unchanged.
+__device__ __forceinline__ void scalar_collision(const float (&f)[27], float (&T)[27], float tauT) {
+  float rho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f, ft = 0.f;
+#pragma unroll
+  for (int q = 0; q < 27; ++q) {
+    rho += f[q];
+    jx += cx(q) * f[q];
+    jy += cy(q) * f[q];
+    jz += cz(q) * f[q];
+    ft += f[q] * T[q];
+  }
+  const float inv_rho = 1.f / rho;
+  const float ux = jx * inv_rho, uy = jy * inv_rho, uz = jz * inv_rho;
+  const float tm = ft * inv_rho;
+  float sx = 0.f, sy = 0.f, sz = 0.f;
+#pragma unroll
+  for (int q = 0; q < 27; ++q) {
+    const float g = f[q] * (T[q] - tm);
+    sx += cx(q) * g;
+    sy += cy(q) * g;
+    sz += cz(q) * g;
+  }
+  const float a = (1.f - 1.f / tauT) * 3.f * inv_rho;
+#pragma unroll
+  for (int q = 0; q < 27; ++q) T[q] = tm + a * ((cx(q) - ux) * sx + (cy(q) - uy) * sy + (cz(q) - uz) * sz);
+}
+
+template <typename S>
+struct ScalarParams {
+  StepParams<S> base;
+  RowIndex<StoreF32> T;    // the scalar populations: FP32 rows at the flow rows' offsets
+  const float* givenT;     // per-cell prescribed concentration (NaN: none), or null
+  float tauT;
+};
+
+// applyLocalCellUpdate with scalar transport (scalarTransportFunctions.h:10-107): T is
+// bounced back with f in solid cells, mirrored with f in free-slip cells, set to the given
+// concentration where one is prescribed, and collided after the flow collision.
+template <typename S>
+__global__ void __launch_bounds__(kStepThreads) step_scalar_kernel(const __grid_constant__ ScalarParams<S> sp) {
+  const StepParams<S>& p = sp.base;
+  const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
+  if (cell >= p.ri.n) return;
+  const uint8_t m = p.marker[cell];
+  const int kind = marker_kind(m);
+  if (kind == kSkip) return;
+  float f[27], T[27];
+  load_cell_ri<S>(p.ri, cell, f);
+  load_cell_ri<StoreF32>(sp.T, cell, T);
+  if (kind == kSolid) {
+#pragma unroll
+    for (int q = 1; q < 27; q += 2) {
+      const float a = f[q], b = T[q];
+      f[q] = f[q + 1];
+      f[q + 1] = a;
+      T[q] = T[q + 1];
+      T[q + 1] = b;
+    }
+  } else {
+    if (kind != kFluid) {
+      apply_boundary(m, f, p.given ? p.given[cell] : p.given_uniform);
+      if (kind == kMirror) bc::mirror(marker_normal(m), T);
+    }
+    if (sp.givenT) {
+      const float tg = sp.givenT[cell];
+      if (tg == tg) {
+#pragma unroll
+        for (int q = 0; q < 27; ++q) T[q] = tg;
+      }
+    }
+    collide<false>(f, p.rx);
+    scalar_collision(f, T, sp.tauT);
+    if (p.health) {
+      const float r = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6];
+      if (!(r > 0.f && r < 1.0e30f)) atomicOr(p.health, 1u);
+    }
+  }
+  store_cell_ri<S>(p.ri, cell, f);
+  store_cell_ri<StoreF32>(sp.T, cell, T);
+}
+
+// Per-cell concentration sum f T / rho (FP64 sums) in logical order.
+template <typename S>
+__global__ void scalar_mean_kernel(GridView<S> g, GridView<StoreF32> t, double* out) {
+  const uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= g.n) return;
+  double rho = 0.0, ft = 0.0;
+#pragma unroll
+  for (int q = 0; q < 27; ++q) {
+    const uint32_t a = shifted(cell, g.shift[q], g.n);
+    const double v = (double)S::load_q(g.fq[q] + a, q);
+    rho += v;
+    ft += v * (double)t.fq[q][a];
+  }
+  out[cell] = ft / rho;
+}
+
+// ------------------------------------------------------------------------------------------
 // set-up kernels (hooks)
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ void cell_ijk(uint32_t cell, const InfoStruct& I, int& i, int& j, int& k) {

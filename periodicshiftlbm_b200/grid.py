@@ -169,6 +169,36 @@ class GridStruct:
         call("psl_get_macroscopic", self._h, out.ctypes.data)
         return out
 
+    # ---- scalar transport (scalarTransportFunctions.h) ----
+    def enableScalarTransport(self, tauT: float):
+        """27 scalar populations T_q streamed with f and collided after it (relaxation tauT)."""
+        call("psl_enable_scalar_transport", self._h, ctypes.c_float(tauT))
+
+    def setScalarGiven(self, givenT: np.ndarray | None):
+        """Per-cell prescribed concentration (NaN: none), or None to remove it."""
+        if givenT is None:
+            call("psl_set_scalar_given_field", self._h, None)
+        else:
+            a = np.ascontiguousarray(givenT, dtype=np.float32).reshape(self.cellCount)
+            call("psl_set_scalar_given_field", self._h, a.ctypes.data)
+
+    @property
+    def TArray(self) -> np.ndarray:
+        out = np.empty((27, self.cellCount), dtype=np.float32)
+        call("psl_get_scalar_populations", self._h, out.ctypes.data)
+        return out
+
+    @TArray.setter
+    def TArray(self, t: np.ndarray):
+        t = np.ascontiguousarray(t, dtype=np.float32).reshape(27, self.cellCount)
+        call("psl_set_scalar_populations", self._h, t.ctypes.data)
+
+    def scalar(self) -> np.ndarray:
+        """Concentration of every cell, sum f T / rho (FP64)."""
+        out = np.empty(self.cellCount, dtype=np.float64)
+        call("psl_get_scalar", self._h, out.ctypes.data)
+        return out
+
     @property
     def shifter(self) -> np.ndarray:
         out = np.zeros(27, dtype=np.int32)

@@ -487,7 +487,7 @@ def run_batch(args):
                 "h2d_bytes_per_step": round(state_bytes / args.steps),
                 "d2h_bytes_per_step": round(state_bytes / args.steps) + 24 * len(cfgs) // max(args.steps, 1),
                 "note": "states uploaded once and downloaded once per run, per-case drag read at the end"},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": 3 * args.steps,
         "clocks": clocks,
     }
     b.close()

@@ -67,6 +67,8 @@ struct psl_batch {
   unsigned long long steps_done = 0;   // host copy of the counter
   std::vector<std::array<uint32_t, 27>> shift0, adv;
   uint32_t tiles = 0;
+  uint32_t* tile_case = nullptr;    // device: case of every tile
+  uint2* offsets = nullptr;         // device: per case and population (offset, limit) of the step
   psl_batch_tuning tuning{};
   cudaGraphExec_t graph = nullptr;
   bool registered = false;          // counted in the member grids' `batched`
@@ -109,6 +111,17 @@ int upload_table(psl_batch* b) {
     tile += (g->n + tc - 1) / tc;
   }
   b->tiles = tile;
+  std::vector<uint32_t> case_of(tile);
+  for (size_t i = 0; i < host.size(); ++i) {
+    const uint32_t end = i + 1 < host.size() ? host[i + 1].tile_begin : tile;
+    for (uint32_t t = host[i].tile_begin; t < end; ++t) case_of[t] = (uint32_t)i;
+  }
+  if (b->tile_case) cudaFree(b->tile_case);
+  b->tile_case = nullptr;
+  BATCH_CUDA(cudaMalloc(&b->tile_case, case_of.size() * sizeof(uint32_t)));
+  BATCH_CUDA(cudaMemcpyAsync(b->tile_case, case_of.data(), case_of.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                             b->stream));
+  if (!b->offsets) BATCH_CUDA(cudaMalloc(&b->offsets, host.size() * 27 * sizeof(uint2)));
   if (!b->table) BATCH_CUDA(cudaMalloc(&b->table, host.size() * sizeof(BatchCase<S>)));
   BATCH_CUDA(cudaMemcpyAsync(b->table, host.data(), host.size() * sizeof(BatchCase<S>), cudaMemcpyHostToDevice,
                              b->stream));
@@ -119,11 +132,14 @@ int upload_table(psl_batch* b) {
 template <typename S>
 void launch_one_step(psl_batch* b) {
   const int threads = b->tuning.threads;
-  const unsigned int blocks =
-      std::max(1u, std::min<unsigned int>(b->tiles, (unsigned int)(b->sms * b->tuning.blocks_per_sm)));
-  batch_step_kernel<S><<<blocks, threads, 0, b->stream>>>(static_cast<const BatchCase<S>*>(b->table),
-                                                           (int)b->grids.size(), b->tiles,
-                                                           (uint32_t)b->tuning.tile_cells, b->step);
+  const unsigned int warps_per_block = (unsigned int)threads / 32;
+  const unsigned int blocks = std::max(
+      1u, std::min<unsigned int>((b->tiles + warps_per_block - 1) / warps_per_block,
+                                 (unsigned int)(b->sms * b->tuning.blocks_per_sm)));
+  const BatchCase<S>* cases = static_cast<const BatchCase<S>*>(b->table);
+  batch_offsets_kernel<S><<<(unsigned int)b->grids.size(), 32, 0, b->stream>>>(cases, b->step, b->offsets);
+  batch_step_kernel<S><<<blocks, threads, 0, b->stream>>>(cases, b->tile_case, b->offsets, b->tiles,
+                                                           (uint32_t)b->tuning.tile_cells);
   batch_advance_kernel<<<1, 1, 0, b->stream>>>(b->step);
 }
 
@@ -164,8 +180,8 @@ int capture_graph(psl_batch* b) {
 int validate_tuning(const psl_batch* b, const psl_batch_tuning& t) {
   BATCH_CHECK(t.threads >= 32 && t.threads <= kBatchMaxThreads && t.threads % 32 == 0, PSL_ERR_INVALID,
               "psl_batch: threads must be a multiple of 32 in [32, 256]");
-  BATCH_CHECK(t.tile_cells >= t.threads && t.tile_cells % t.threads == 0 && t.tile_cells <= (1 << 20), PSL_ERR_INVALID,
-              "psl_batch: tile_cells must be a multiple of threads, at most 2^20");
+  BATCH_CHECK(t.tile_cells >= 32 && t.tile_cells % 32 == 0 && t.tile_cells <= (1 << 20), PSL_ERR_INVALID,
+              "psl_batch: tile_cells (cells per warp tile) must be a multiple of 32, at most 2^20");
   BATCH_CHECK(t.blocks_per_sm >= 1 && t.blocks_per_sm <= 64, PSL_ERR_INVALID, "psl_batch: blocks_per_sm out of range");
   int per_sm = 0;
   int rc = with_batch_storage(b->storage, [&](auto s) { return occupancy<decltype(s)>(t.threads, &per_sm); });
@@ -245,7 +261,7 @@ int psl_batch_create(psl_grid* const* grids, int count, psl_batch** out) {
   }
   psl_batch_tuning t{};
   t.threads = 128;
-  t.tile_cells = 512;
+  t.tile_cells = 256;
   int per_sm = 0;
   int rc = with_batch_storage(b->storage, [&](auto s) { return occupancy<decltype(s)>(t.threads, &per_sm); });
   t.blocks_per_sm = std::max(1, per_sm);
@@ -266,6 +282,8 @@ int psl_batch_destroy(psl_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   drop_graph(b);
   if (b->table) cudaFree(b->table);
+  if (b->tile_case) cudaFree(b->tile_case);
+  if (b->offsets) cudaFree(b->offsets);
   if (b->step) cudaFree(b->step);
   if (b->done) cudaEventDestroy(b->done);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -349,7 +367,7 @@ int psl_batch_autotune(psl_batch* b, int trial_steps, psl_batch_tuning* chosen) 
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
   const int thread_options[] = {64, 128, 256};
-  const int tile_factors[] = {1, 2, 4, 8, 16};
+  const int tile_factors[] = {1, 2, 4, 8, 16, 32};  // warp tiles of 32 x factor cells
   for (int threads : thread_options) {
     int per_sm = 0;
     rc = with_batch_storage(b->storage, [&](auto s) { return occupancy<decltype(s)>(threads, &per_sm); });
@@ -359,7 +377,7 @@ int psl_batch_autotune(psl_batch* b, int trial_steps, psl_batch_tuning* chosen) 
       for (int tf : tile_factors) {
         psl_batch_tuning t{};
         t.threads = threads;
-        t.tile_cells = threads * tf;
+        t.tile_cells = 32 * tf;
         t.blocks_per_sm = resident[r];
         if (apply_tuning(b, t)) continue;
         with_batch_storage(b->storage, [&](auto s) {

@@ -2,11 +2,11 @@
 // size and Reynolds number) advanced by ONE persistent kernel per step.
 //
 // Work decomposition: each case's cells are cut into tiles of `tile_cells` consecutive
-// cells; the tiles of all cases form one index space that a grid of resident CTAs walks
-// with a fixed stride (CTA b takes tiles b, b + gridDim, ...).  At the start of a tile the
-// CTA finds the tile's case (binary search over the cases' first tiles), and threads 0-26
-// derive the case's 27 row offsets for the current step into shared memory; every thread
-// then updates cells of the tile exactly as the single-grid update kernel does
+// cells; the tiles of all cases form one index space that the resident warps walk with a
+// fixed stride (warp w takes tiles w, w + warps, ...).  A table gives each tile's case; a
+// small kernel before the update writes every case's 27 row offsets for the step, which
+// lanes 0-26 copy into the warp's shared-memory slot at the start of a tile; every lane then
+// updates cells of the tile exactly as the single-grid update kernel does
 // (applyLocalCellUpdate.h:1-74).
 //
 // The periodic shifts are not kernel parameters: after s applications of applyStreaming
@@ -38,6 +38,25 @@ struct BatchCase {
 
 constexpr int kBatchMaxThreads = 256;
 
+// Rows of a tile that no population's wrap point cuts: population Q of `cell` is at
+// base[cell + adj[Q]] with a tile-uniform adj (no per-cell compare).
+template <typename S, int Q = 0>
+__device__ __forceinline__ void load_cell_adj(typename S::type* base, const uint32_t (&adj)[27], uint32_t cell,
+                                              float (&f)[27]) {
+  if constexpr (Q < 27) {
+    f[Q] = S::template load_once<Q>(base + (cell + adj[Q]));
+    load_cell_adj<S, Q + 1>(base, adj, cell, f);
+  }
+}
+template <typename S, int Q = 0>
+__device__ __forceinline__ void store_cell_adj(typename S::type* base, const uint32_t (&adj)[27], uint32_t cell,
+                                               const float (&f)[27]) {
+  if constexpr (Q < 27) {
+    S::template store_once<Q>(base + (cell + adj[Q]), f[Q]);
+    store_cell_adj<S, Q + 1>(base, adj, cell, f);
+  }
+}
+
 // Shift of population q at step `step`: (shift0 + step * adv) mod n, in 64-bit arithmetic
 // (step mod n < 2^31 and adv < 2^31, so the product fits).
 __device__ __forceinline__ uint32_t batch_shift(uint32_t shift0, uint32_t adv, uint32_t n, unsigned long long step) {
@@ -45,56 +64,86 @@ __device__ __forceinline__ uint32_t batch_shift(uint32_t shift0, uint32_t adv, u
   return (uint32_t)((s * adv + shift0) % n);
 }
 
+// Per step, before the update: every case's 27 row offsets and wrap limits for the shifts
+// after step + 1 streamings (one block per case, one thread per population).
 template <typename S>
-__global__ void __launch_bounds__(kBatchMaxThreads) batch_step_kernel(const BatchCase<S>* __restrict__ cases, int ncases,
-                                                                      uint32_t tiles, uint32_t tile_cells,
-                                                                      const unsigned long long* __restrict__ step) {
-  // the current tile's case: row offsets and scalars live in shared memory, so the cell
-  // loop holds no per-case registers
-  __shared__ RowIndex<S> ri;
-  __shared__ int s_case;
-  __shared__ RelaxationT<float> s_rx;
-  __shared__ float4 s_given_uniform;
-  __shared__ const uint8_t* s_marker;
-  __shared__ const float4* s_given;
-  __shared__ unsigned int* s_health;
-  const unsigned long long st = *step;
-  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    __syncthreads();  // the previous tile's readers of `ri` are done
-    if (threadIdx.x < 27) {
-      int lo = 0, hi = ncases - 1;  // last case whose first tile is <= tile
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (cases[mid].tile_begin <= tile) lo = mid;
-        else hi = mid - 1;
-      }
-      const BatchCase<S>& c = cases[lo];
-      const int q = threadIdx.x;
-      const uint32_t sh = batch_shift(c.shift0[q], c.adv[q], c.n, st + 1);
-      ri.off[q] = (uint32_t)q * c.stride + sh;
-      ri.lim[q] = c.n - sh;
-      if (q == 0) {
-        ri.base = c.f;
-        ri.n = c.n;
-        s_case = lo;
-        s_rx = c.rx;
-        s_given_uniform = c.given_uniform;
-        s_marker = c.marker;
-        s_given = c.given;
-        s_health = c.health;
-      }
+__global__ void batch_offsets_kernel(const BatchCase<S>* __restrict__ cases, const unsigned long long* __restrict__ step,
+                                     uint2* __restrict__ offsets) {
+  const int c = blockIdx.x, q = threadIdx.x;
+  if (q >= 27) return;
+  const BatchCase<S>& bc = cases[c];
+  const uint32_t sh = batch_shift(bc.shift0[q], bc.adv[q], bc.n, *step + 1);
+  offsets[c * 27 + q] = make_uint2((uint32_t)q * bc.stride + sh, bc.n - sh);
+}
+
+// Warp tiles: every warp walks its own tiles of `tile_cells` consecutive cells (warp w of
+// the grid takes tiles w, w + warps, ...) with its case data in its own shared-memory slot,
+// so warps synchronise only within themselves (no CTA barrier couples them).
+struct BatchWarpSlot {
+  uint32_t off[27];
+  uint32_t lim[27];
+  uint32_t adj[27];  // tile-uniform offsets when no wrap point cuts the tile
+};
+
+template <typename S>
+__global__ void __launch_bounds__(kBatchMaxThreads, 4) batch_step_kernel(const BatchCase<S>* __restrict__ cases,
+                                                                         const uint32_t* __restrict__ tile_case,
+                                                                         const uint2* __restrict__ offsets,
+                                                                         uint32_t tiles, uint32_t tile_cells) {
+  __shared__ BatchWarpSlot slots[kBatchMaxThreads / 32];
+  const int lane = threadIdx.x & 31;
+  BatchWarpSlot& slot = slots[threadIdx.x >> 5];
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t tile = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); tile < tiles; tile += warps) {
+    const uint32_t ci = tile_case[tile];
+    const BatchCase<S>& c = cases[ci];
+    const uint32_t n = c.n;
+    const uint32_t first = (tile - c.tile_begin) * tile_cells;
+    const uint32_t last = min(first + tile_cells, n);
+    bool cut = false;
+    __syncwarp();  // the previous tile's readers of the slot are done
+    if (lane < 27) {
+      const uint2 ol = offsets[ci * 27 + lane];
+      slot.off[lane] = ol.x;
+      slot.lim[lane] = ol.y;
+      slot.adj[lane] = ol.x - (first >= ol.y ? n : 0u);
+      cut = first < ol.y && last - 1 >= ol.y;
     }
-    __syncthreads();
-    const uint32_t first = (tile - cases[s_case].tile_begin) * tile_cells;
-    const uint32_t last = min(first + tile_cells, ri.n);
-    for (uint32_t cell = first + threadIdx.x; cell < last; cell += blockDim.x) {
-      const uint8_t m = s_marker[cell];
+    const bool any_cut = __any_sync(0xffffffffu, cut);  // also orders the slot writes
+    typename S::type* base = c.f;
+    const uint8_t* marker = c.marker;
+    for (uint32_t cell = first + lane; cell < last; cell += 32) {
+      const uint8_t m = marker[cell];
       const int kind = marker_kind(m);
       if (kind == kSkip) continue;
       float f[27];
-      load_cell_ri<S>(ri, cell, f);
-      local_cell_update(kind, m, f, s_given, s_given_uniform, cell, s_rx, s_health);
-      store_cell_ri<S>(ri, cell, f);
+      if (!any_cut) {
+        load_cell_adj<S>(base, slot.adj, cell, f);
+      } else {
+        RowIndex<S> ri;
+        ri.base = base;
+        ri.n = n;
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+          ri.off[q] = slot.off[q];
+          ri.lim[q] = slot.lim[q];
+        }
+        load_cell_ri<S>(ri, cell, f);
+      }
+      local_cell_update(kind, m, f, c.given, c.given_uniform, cell, c.rx, c.health);
+      if (!any_cut) {
+        store_cell_adj<S>(base, slot.adj, cell, f);
+      } else {
+        RowIndex<S> ri;
+        ri.base = base;
+        ri.n = n;
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+          ri.off[q] = slot.off[q];
+          ri.lim[q] = slot.lim[q];
+        }
+        store_cell_ri<S>(ri, cell, f);
+      }
     }
   }
 }

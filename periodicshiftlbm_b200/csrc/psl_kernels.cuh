@@ -63,7 +63,7 @@ struct StepParams {
 // The boundary branch runs for ~2% of cells; keeping it out of line keeps the hot path's
 // instruction footprint small.  (applyLocalCellUpdate.h:41-67)
 template <typename T>
-static __device__ __noinline__ void apply_boundary(uint8_t m, T (&f)[27], float4 given) {
+static __device__ __noinline__ void apply_boundary_out_of_line(uint8_t m, T (&f)[27], float4 given) {
   const int kind = marker_kind(m), normal = marker_normal(m);
   T rho = given.x, ux = given.y, uy = given.z, uz = given.w;
   if (kind == kMirror) {
@@ -74,6 +74,19 @@ static __device__ __noinline__ void apply_boundary(uint8_t m, T (&f)[27], float4
   else if (kind == kGivenU) bc::restore_rho(normal, f, rho, ux, uy, uz);
   else if (kind == kGivenNone) bc::restore_rho_u(normal, f, rho, ux, uy, uz);
   bc::mbbc(normal, f, rho, ux, uy, uz);
+}
+
+// The call site: the populations go to a local copy inside the boundary branch only.  Passing
+// the caller's own array by reference would take its address, and nvcc then keeps it in
+// local memory for every cell (a stack write of all 27 populations per fluid cell too).
+template <typename T>
+__device__ __forceinline__ void apply_boundary(uint8_t m, T (&f)[27], float4 given) {
+  T copy[27];
+#pragma unroll
+  for (int q = 0; q < 27; ++q) copy[q] = f[q];
+  apply_boundary_out_of_line(m, copy, given);
+#pragma unroll
+  for (int q = 0; q < 27; ++q) f[q] = copy[q];
 }
 
 template <typename S, int Q = 0>

@@ -624,8 +624,11 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
       k = 2 + r / nx;
       i = r % nx;
     } else {
-      const uint32_t u = t - zl - yl, layer = u / ((ny - 4) * (nz - 4)), r = u % ((ny - 4) * (nz - 4));
-      i = layer < 2 ? layer : nx - 4 + layer;
+      // x faces: lanes 2m and 2m+1 take the two cells of one row (i and i+1, the same coarse
+      // parent), so each store covers 8 contiguous bytes instead of 4 bytes of a line
+      const uint32_t u = t - zl - yl, per_side = 2u * (ny - 4) * (nz - 4);
+      const uint32_t side = u / per_side, w = u % per_side, r = w >> 1;
+      i = (side ? nx - 2 : 0) + (int)(w & 1u);
       j = 2 + r % (ny - 4);
       k = 2 + r / (ny - 4);
     }

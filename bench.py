@@ -147,6 +147,24 @@ def hbm_peak():
         return 6650.0, "fallback"
 
 
+def closure_kernel() -> tuple:
+    """(kernel name, label) of the learned-closure update the library runs: the per-warp
+    MMA kernel unless PSL_CLOSURE_PATH=tcgen05 selects the CTA-wide tcgen05 one."""
+    if os.environ.get("PSL_CLOSURE_PATH") == "tcgen05":
+        return "step_learned_kernel", "tcgen05, CTA-wide"
+    return "step_learned_warp_kernel", "per-warp MMA"
+
+
+def batch_traffic(storage: str, cells: int):
+    """DRAM bytes per launch of the batched update: the per-cell traffic of the committed
+    16-case capture (profiles/batch_step_kernel_batch16.md, FP32) times the cells."""
+    path = os.path.join(REPO, "profiles", "batch_step_kernel_batch16.md")
+    if storage != "f32" or not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_cell:\s*([0-9.eE+]+)", open(path).read())
+    return round(float(m.group(1)) * cells) if m else None
+
+
 def ncu_traffic(kernel: str, storage: str):
     """dram bytes read+written per launch of the coarse update kernel from the committed
     ncu summary (profiles/<kernel>_<storage>_sphere512.md), or None."""
@@ -304,20 +322,20 @@ def run_native(args):
             "storage": args.storage,
             "updates_per_step": updates,
             "reference_formula_updates_per_step": cfg.reference_updates_per_step(),
-            "collision": ("cumulant + learned MLP closure (tcgen05)" if args.sgs == "mlp" else
+            "collision": (f"cumulant + learned MLP closure ({closure_kernel()[1]})" if args.sgs == "mlp" else
                           "cumulant + Smagorinsky" if cfg.smagorinsky else "cumulant"),
             "l2": "inputs larger than L2 (no flush)" if cfg.refine else "state fits partly in L2",
             "parallelism": f"replicas x{world}",
         },
         "roofline": {
             "bound": "hbm",
-            "kernel": "step_learned_kernel (coarse grid)" if args.sgs == "mlp" else "step_kernel (coarse grid)",
+            "kernel": (closure_kernel()[0] if args.sgs == "mlp" else "step_kernel") + " (coarse grid)",
             "achieved": round(achieved, 1),
             "peak": peak,
             "peak_kind": peak_kind,
             "unit": "GB/s",
             "frac": round(achieved / peak, 4),
-            "traffic": ncu_traffic("step_learned_kernel" if args.sgs == "mlp" else "step_kernel", args.storage),
+            "traffic": ncu_traffic(closure_kernel()[0] if args.sgs == "mlp" else "step_kernel", args.storage),
             "algorithmic_bytes_per_launch": coarse_bytes,
             "launch_ms": round(coarse_ms, 4),
             "fine_launch_ms": round(fine_ms, 4) if fine_ms else None,
@@ -481,7 +499,8 @@ def run_batch(args):
                    "storage": args.storage, "tuning": tuning, "graph": "one step per replay",
                    "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "kernel": "batch_step_kernel", "achieved": round(achieved, 1), "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": batch_traffic(args.storage, cells),
                      "algorithmic_bytes_per_launch": bpu * cells},
         "e2e": {"value": round(cells * args.steps * world / e_s / 1e6, 1), "unit": "MLUPS",
                 "h2d_bytes_per_step": round(state_bytes / args.steps),

@@ -282,7 +282,8 @@ typedef struct psl_batch psl_batch;
 typedef struct psl_batch_tuning {
   int threads;       /* threads per CTA: a multiple of 32, at most 256 */
   int tile_cells;    /* consecutive cells per warp tile: a multiple of 32 */
-  int blocks_per_sm; /* resident CTAs per SM in the persistent grid */
+  int blocks_per_sm; /* resident CTAs per SM in the persistent grid; 0: a grid of as many
+                        CTAs as the tiles need (each warp's tile loop then runs once) */
   float ms_per_step; /* time per step measured by psl_batch_autotune (0 if not tuned) */
 } psl_batch_tuning;
 int psl_batch_create(psl_grid* const* grids, int count, psl_batch** out);
@@ -296,7 +297,7 @@ int psl_batch_get_stream(const psl_batch* batch, void** stream);
 int psl_batch_get_tuning(const psl_batch* batch, psl_batch_tuning* tuning);
 int psl_batch_set_tuning(psl_batch* batch, const psl_batch_tuning* tuning);
 /* Project-written autotuner: times every candidate launch shape (threads 64/128/256 x
- * warp tiles of 32-1024 cells x {max, max/2} resident CTAs per SM) over `trial_steps` steps on the
+ * warp tiles of 32-1024 cells x {max, max/2, 0} CTAs per SM) over `trial_steps` steps on the
  * batch itself, adopts the fastest and reports it in *chosen.  The populations and the
  * step counter are saved first and restored afterwards, so tuning does not advance the
  * simulation. */

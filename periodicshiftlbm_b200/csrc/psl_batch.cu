@@ -133,9 +133,10 @@ template <typename S>
 void launch_one_step(psl_batch* b) {
   const int threads = b->tuning.threads;
   const unsigned int warps_per_block = (unsigned int)threads / 32;
-  const unsigned int blocks = std::max(
-      1u, std::min<unsigned int>((b->tiles + warps_per_block - 1) / warps_per_block,
-                                 (unsigned int)(b->sms * b->tuning.blocks_per_sm)));
+  const unsigned int all_tiles = std::max(1u, (b->tiles + warps_per_block - 1) / warps_per_block);
+  const unsigned int blocks =
+      b->tuning.blocks_per_sm == 0 ? all_tiles
+                                   : std::min(all_tiles, (unsigned int)(b->sms * b->tuning.blocks_per_sm));
   const BatchCase<S>* cases = static_cast<const BatchCase<S>*>(b->table);
   batch_offsets_kernel<S><<<(unsigned int)b->grids.size(), 32, 0, b->stream>>>(cases, b->step, b->offsets);
   batch_step_kernel<S><<<blocks, threads, 0, b->stream>>>(cases, b->tile_case, b->offsets, b->tiles,
@@ -182,7 +183,7 @@ int validate_tuning(const psl_batch* b, const psl_batch_tuning& t) {
               "psl_batch: threads must be a multiple of 32 in [32, 256]");
   BATCH_CHECK(t.tile_cells >= 32 && t.tile_cells % 32 == 0 && t.tile_cells <= (1 << 20), PSL_ERR_INVALID,
               "psl_batch: tile_cells (cells per warp tile) must be a multiple of 32, at most 2^20");
-  BATCH_CHECK(t.blocks_per_sm >= 1 && t.blocks_per_sm <= 64, PSL_ERR_INVALID, "psl_batch: blocks_per_sm out of range");
+  BATCH_CHECK(t.blocks_per_sm >= 0 && t.blocks_per_sm <= 64, PSL_ERR_INVALID, "psl_batch: blocks_per_sm out of range");
   int per_sm = 0;
   int rc = with_batch_storage(b->storage, [&](auto s) { return occupancy<decltype(s)>(t.threads, &per_sm); });
   if (rc) return rc;
@@ -372,8 +373,9 @@ int psl_batch_autotune(psl_batch* b, int trial_steps, psl_batch_tuning* chosen) 
     int per_sm = 0;
     rc = with_batch_storage(b->storage, [&](auto s) { return occupancy<decltype(s)>(threads, &per_sm); });
     if (rc || per_sm < 1) continue;
-    const int resident[] = {per_sm, std::max(1, per_sm / 2)};
-    for (int r = 0; r < (per_sm > 1 ? 2 : 1); ++r)
+    // resident grids of per_sm and per_sm/2 CTAs per SM, and (0) one CTA per tiles' worth
+    const int resident[] = {per_sm, std::max(1, per_sm / 2), 0};
+    for (int r = 0; r < 3; ++r)
       for (int tf : tile_factors) {
         psl_batch_tuning t{};
         t.threads = threads;

@@ -31,7 +31,8 @@ def solo_state(cfg, steps):
 
 @pytest.mark.parametrize("tuning", [None, {"threads": 64, "tile_cells": 64, "blocks_per_sm": 4},
                                     {"threads": 256, "tile_cells": 1024, "blocks_per_sm": 2},
-                                    {"threads": 128, "tile_cells": 96, "blocks_per_sm": 3}])
+                                    {"threads": 128, "tile_cells": 96, "blocks_per_sm": 3},
+                                    {"threads": 128, "tile_cells": 64, "blocks_per_sm": 0}])
 def test_batched_equals_solo_runs(tuning):
     cfgs = small_configs()
     grids, cases = make_batch_grids(cfgs)

@@ -91,7 +91,8 @@ __global__ void __launch_bounds__(kStepThreads, 7) step_learned_warp_kernel(cons
     int4* dst = reinterpret_cast<int4*>(&w);
     for (int i = threadIdx.x; i < (int)(sizeof(MlpWarp) / 16); i += blockDim.x) dst[i] = src[i];
   }
-  __syncthreads();
+  // (the barrier that publishes the weights comes after the cell's loads and moments, so the
+  // weight copy overlaps them)
   __half* xt = xtile[threadIdx.x >> 5];
   {
     const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
@@ -117,7 +118,7 @@ __global__ void __launch_bounds__(kStepThreads, 7) step_learned_warp_kernel(cons
         mlp_features(K[2][0][0], K[0][2][0], K[0][0][2], K[1][1][0], K[1][0][1], K[0][1][1], rho, inv_rho, p.width, x);
       }
     }
-    __syncwarp();
+    __syncthreads();  // weights in shared memory; reached by every thread of the CTA
     const float nu_t = mlp_warp_eval(w, xt, x);
     if (kind != kSkip && kind != kSolid) {
       relax_rebuild(f, K, rho, ux, uy, uz, inv_rho, 1.f / (3.f * (p.nu + nu_t) + 0.5f));

@@ -20,8 +20,8 @@ def small_configs():
     return out
 
 
-def solo_state(cfg, steps):
-    grids, case = make_sphere_grids(cfg)
+def solo_state(cfg, steps, storage="f32"):
+    grids, case = make_sphere_grids(cfg, storage=storage)
     for _ in range(steps):
         updateGrid(grids, 0)
     out = (grids[0].fArray, grids[0].shifter, getSphereDrag(grids[0], case))
@@ -66,6 +66,24 @@ def test_autotune_keeps_state_and_picks_a_valid_shape():
     for cfg, g in zip(cfgs, grids):
         f, s, _ = solo_state(cfg, 8)
         assert np.array_equal(g.fArray, f), cfg.name
+    b.close()
+    for g in grids:
+        g.close()
+
+
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+def test_batched_16bit_storage_equals_solo_runs(storage):
+    """The 16-bit f - w forms batch like FP32: each grid bit for bit as its own run."""
+    cfgs = small_configs()[:3]
+    grids, cases = make_batch_grids(cfgs, storage=storage)
+    b = Batch(grids)
+    b.tuning = {"threads": 128, "tile_cells": 64, "blocks_per_sm": 0}
+    b.run(9)
+    for cfg, g, c in zip(cfgs, grids, cases):
+        f, s, d = solo_state(cfg, 9, storage)
+        assert np.array_equal(g.shifter, s), cfg.name
+        assert np.array_equal(g.fArray, f), cfg.name
+        assert getSphereDrag(g, c) == d
     b.close()
     for g in grids:
         g.close()

@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(kBatchMaxThreads, 4) batch_step_kernel(const B
         }
         load_cell_ri<S>(ri, cell, f);
       }
-      local_cell_update(kind, m, f, c.given, c.given_uniform, cell, c.rx, c.health);
+      local_cell_update<kBatchMaxThreads>(kind, m, f, c.given, c.given_uniform, cell, c.rx, c.health);
       if (!any_cut) {
         store_cell_adj<S>(base, slot.adj, cell, f);
       } else {

@@ -63,7 +63,8 @@ struct StepParams {
 // The boundary branch runs for ~2% of cells; keeping it out of line keeps the hot path's
 // instruction footprint small.  (applyLocalCellUpdate.h:41-67)
 template <typename T>
-static __device__ __noinline__ void apply_boundary_out_of_line(uint8_t m, T (&f)[27], float4 given) {
+static __device__ __noinline__ void apply_boundary_out_of_line(uint8_t m, T* populations, float4 given) {
+  T (&f)[27] = *reinterpret_cast<T(*)[27]>(populations);
   const int kind = marker_kind(m), normal = marker_normal(m);
   T rho = given.x, ux = given.y, uy = given.z, uz = given.w;
   if (kind == kMirror) {
@@ -76,17 +77,21 @@ static __device__ __noinline__ void apply_boundary_out_of_line(uint8_t m, T (&f)
   bc::mbbc(normal, f, rho, ux, uy, uz);
 }
 
-// The call site: the populations go to a local copy inside the boundary branch only.  Passing
-// the caller's own array by reference would take its address, and nvcc then keeps it in
-// local memory for every cell (a stack write of all 27 populations per fluid cell too).
-template <typename T>
+// The call site: the populations go through the thread's own slot in shared memory
+// (kSlots >= the block's threads), written and read inside the boundary branch only.
+// Passing the caller's array by reference would take its address, and nvcc then keeps it in
+// local memory for every cell (a stack write of all 27 populations per fluid cell too); a
+// copy in local memory inside the branch still cost a warp holding one inflow cell 8% of the
+// update launch on a 512-wide grid, the shared-memory slot 3%.
+template <int kSlots = kStepThreads, typename T>
 __device__ __forceinline__ void apply_boundary(uint8_t m, T (&f)[27], float4 given) {
-  T copy[27];
+  __shared__ T slot[kSlots][27];
+  T* mine = slot[threadIdx.x];
 #pragma unroll
-  for (int q = 0; q < 27; ++q) copy[q] = f[q];
-  apply_boundary_out_of_line(m, copy, given);
+  for (int q = 0; q < 27; ++q) mine[q] = f[q];
+  apply_boundary_out_of_line(m, mine, given);
 #pragma unroll
-  for (int q = 0; q < 27; ++q) f[q] = copy[q];
+  for (int q = 0; q < 27; ++q) f[q] = mine[q];
 }
 
 template <typename S, int Q = 0>
@@ -125,7 +130,7 @@ __device__ __forceinline__ void store_cell_ri(const RowIndex<S>& r, uint32_t cel
 
 // The per-cell body (applyLocalCellUpdate.h:21-72): bounce-back for solid cells; for the
 // others the boundary condition of the marker, the collision and a density health check.
-template <typename T>
+template <int kSlots = kStepThreads, typename T>
 __device__ __forceinline__ void local_cell_update(int kind, uint8_t m, T (&f)[27], const float4* given, float4 given_uniform,
                                                   uint32_t cell, const RelaxationT<T>& rx, unsigned int* health) {
   if (kind == kSolid) {
@@ -136,7 +141,7 @@ __device__ __forceinline__ void local_cell_update(int kind, uint8_t m, T (&f)[27
       f[q + 1] = t;
     }
   } else {
-    if (kind != kFluid) apply_boundary(m, f, given ? given[cell] : given_uniform);
+    if (kind != kFluid) apply_boundary<kSlots>(m, f, given ? given[cell] : given_uniform);
     collide<false>(f, rx);
     if (health) {
       const T r = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6];

@@ -97,16 +97,13 @@ int launch(psl_grid* g) {
   // PSL_CLOSURE_PATH=tcgen05 selects the CTA-wide tcgen05 evaluation; default per warp
   const char* path_env = getenv("PSL_CLOSURE_PATH");
   const bool cta_path = path_env && std::string(path_env) == "tcgen05";
-  int sms = 0, per_sm = 0;
-  MLP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+  int per_sm = 0;  // one tile per CTA; the check only refuses a kernel that cannot be resident
   if (cta_path)
     MLP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_learned_kernel<S>, kMlpRows, 0));
   else
     MLP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_learned_warp_kernel<S>, kStepThreads, 0));
   if (per_sm < 1) return fail(PSL_ERR_CUDA, "learned update: kernel cannot be resident");
   const unsigned int tiles = (g->n + kMlpRows - 1) / kMlpRows;
-  const unsigned int blocks = std::min<unsigned int>(tiles, (unsigned int)(sms * per_sm));
-  (void)blocks;
   if (cta_path)
     step_learned_kernel<S><<<tiles, kMlpRows, 0, g->stream>>>(p);
   else

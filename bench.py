@@ -68,6 +68,26 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
+def max_over_ranks(x: float, world: int) -> float:
+    """The largest x over the ranks of the process group (x itself on one rank): the job's
+    time is its slowest rank's.  Runs on the group's own device (CUDA for NCCL, host for gloo)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank_step: float, steps: int, world: int, ms: float) -> float:
+    """Whole-job throughput in millions of units per second: every rank (an independent
+    replica) processes `units_per_rank_step` units per step, in the slowest rank's `ms`."""
+    return units_per_rank_step * steps * world / (ms * 1e-3) / 1e6
+
+
 # ------------------------------------------------------------------------------------------
 # clocks sampled during the timed region
 # ------------------------------------------------------------------------------------------
@@ -251,15 +271,9 @@ def run_native(args):
     torch.cuda.synchronize()
     clocks = sampler.stop()
     barrier()
-    ms = t0.elapsed_time(t1)
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(t0.elapsed_time(t1), world)
     updates = cfg.updates_per_step()
-    value = updates * args.steps * world / (ms * 1e-3) / 1e6
+    value = job_rate(updates, args.steps, world, ms)
 
     # roofline of the dominant kernel: the coarse-grid update
     coarse_ms = statistics.mean(a.elapsed_time(b) for a, b in ev["coarse"])
@@ -292,15 +306,9 @@ def run_native(args):
     for g, h in zip(grids, pinned_out):
         g.read_populations(h.numpy())
     torch.cuda.synchronize()
-    e_s = time.perf_counter() - e0
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_s = float(t.item())
+    e_s = max_over_ranks(time.perf_counter() - e0, world)
     state_bytes = sum(h.nbytes for h in host_state)
-    e2e_value = updates * args.steps * world / e_s / 1e6
+    e2e_value = job_rate(updates, args.steps, world, e_s * 1e3)
 
     line = {
         "metric": METRIC,
@@ -465,12 +473,8 @@ def run_batch(args):
     t1.record(stream)
     b.synchronize()
     clocks = sampler.stop()
-    ms = t0.elapsed_time(t1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = cells * args.steps * world / (ms * 1e-3) / 1e6
+    ms = max_over_ranks(t0.elapsed_time(t1), world)
+    value = job_rate(cells, args.steps, world, ms)
     bpu = BYTES_PER_UPDATE[args.storage]
     peak, peak_kind = hbm_peak()
     achieved = bpu * cells / (ms / args.steps * 1e-3) / 1e9
@@ -488,7 +492,7 @@ def run_batch(args):
     drags = [float(getSphereForce(g, c)[0]) for g, c in zip(grids, cases)]
     for g, h in zip(grids, pinned):
         g.read_populations(h.numpy())
-    e_s = time.perf_counter() - e0
+    e_s = max_over_ranks(time.perf_counter() - e0, world)
     state_bytes = sum(h.numpy().nbytes for h in pinned)
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
@@ -502,7 +506,7 @@ def run_batch(args):
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": batch_traffic(args.storage, cells),
                      "algorithmic_bytes_per_launch": bpu * cells},
-        "e2e": {"value": round(cells * args.steps * world / e_s / 1e6, 1), "unit": "MLUPS",
+        "e2e": {"value": round(job_rate(cells, args.steps, world, e_s * 1e3), 1), "unit": "MLUPS",
                 "h2d_bytes_per_step": round(state_bytes / args.steps),
                 "d2h_bytes_per_step": round(state_bytes / args.steps) + 24 * len(cfgs) // max(args.steps, 1),
                 "note": "states uploaded once and downloaded once per run, per-case drag read at the end"},

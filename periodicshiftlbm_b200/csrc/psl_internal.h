@@ -53,6 +53,7 @@ struct psl_grid {
   float tauT = 1.f;
   void* mlp = nullptr;              // learned closure (psl::MlpDevice), or null: Smagorinsky
   float mlp_width = 1.f;            // filter width fed to the closure
+  float mlp_scalars[24] = {};       // its normalisation, b3, output scale (psl::MlpScalars)
 };
 
 // Launches the update kernel with the learned closure (psl_learned.cu); status as psl_*.

@@ -29,24 +29,53 @@ int fail(int code, const std::string& msg) {
 // The grid's closure buffer: the tcgen05 layout followed by the per-warp layout.
 struct MlpBoth {
   MlpDevice cta;
-  MlpWarp warp;
+  MlpFrag warp;
 };
+static_assert(sizeof(MlpScalars) <= sizeof(float) * 24, "psl_grid::mlp_scalars holds MlpScalars");
 
-// Per-warp layout: W[out][in] FP16 rows (padded), FP32 biases and normalisation.
-void pack_warp(const psl_sgs_mlp& m, MlpWarp& d) {
+// FP16 pair (lo, hi) as one 32-bit fragment register.
+uint32_t half_pair(float lo, float hi) {
+  const __half a = __float2half_rn(lo), b = __float2half_rn(hi);
+  uint16_t ua, ub;
+  std::memcpy(&ua, &a, 2);
+  std::memcpy(&ub, &b, 2);
+  return (uint32_t)ua | ((uint32_t)ub << 16);
+}
+
+// Per-warp layout: every lane's B fragments in the order mlp_warp_eval loads them
+// (psl_mlp_warp.cuh); W(o, k) gives the weight of output o, input k.
+template <typename Wfn>
+uint4 frag_pair(Wfn W, int np, int kk, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  auto b0 = [&](int nt) { return half_pair(W(8 * nt + g, 16 * kk + 2 * t), W(8 * nt + g, 16 * kk + 2 * t + 1)); };
+  auto b1 = [&](int nt) { return half_pair(W(8 * nt + g, 16 * kk + 8 + 2 * t), W(8 * nt + g, 16 * kk + 9 + 2 * t)); };
+  return make_uint4(b0(2 * np), b1(2 * np), b0(2 * np + 1), b1(2 * np + 1));
+}
+
+void pack_warp(const psl_sgs_mlp& m, MlpFrag& d, MlpScalars& sc) {
   std::memset(&d, 0, sizeof(d));
-  for (int o = 0; o < 32; ++o) {
-    for (int k = 0; k < kMlpIn; ++k) d.w1[o * kW1Stride + k] = __float2half_rn(m.w1[o][k]);
-    d.w1[o * kW1Stride + kMlpIn] = __float2half_rn(m.b1[o]);  // times the constant input 1
-    for (int k = 0; k < 32; ++k) d.w2[o * kW2Stride + k] = __float2half_rn(m.w2[o][k]);
-    d.b2[o] = m.b2[o];
+  auto w1 = [&](int o, int k) { return k < kMlpIn ? m.w1[o][k] : (k == kMlpIn ? m.b1[o] : 0.f); };
+  auto w2 = [&](int o, int k) { return m.w2[o][k]; };
+  auto w3 = [&](int o, int k) { return o == 0 ? m.w3[k] : 0.f; };
+  for (int lane = 0; lane < 32; ++lane) {
+    const int t = lane & 3;
+    for (int np = 0; np < 2; ++np) {
+      d.w1[np][lane] = frag_pair(w1, np, 0, lane);
+      for (int kk = 0; kk < 2; ++kk) d.w2[kk][np][lane] = frag_pair(w2, np, kk, lane);
+    }
+    const uint4 k0 = frag_pair(w3, 0, 0, lane), k1 = frag_pair(w3, 0, 1, lane);
+    d.w3[lane] = make_uint4(k0.x, k0.y, k1.x, k1.y);  // N-tile 0 of K-steps 0 and 1
+    for (int kk = 0; kk < 2; ++kk) {
+      const int c = 16 * kk + 2 * t;
+      d.b2[kk][lane] = make_float4(m.b2[c], m.b2[c + 1], m.b2[c + 8], m.b2[c + 9]);
+    }
   }
-  for (int k = 0; k < 32; ++k) d.w3[k] = __float2half_rn(m.w3[k]);  // row 0
-  d.b3 = m.b3;
-  d.out_scale = m.out_scale;
+  std::memset(&sc, 0, sizeof(sc));
+  sc.b3 = m.b3;
+  sc.out_scale = m.out_scale;
   for (int i = 0; i < kMlpIn; ++i) {
-    d.in_scale[i] = m.in_scale[i];
-    d.in_offset[i] = -m.in_shift[i] * m.in_scale[i];
+    sc.in_scale[i] = m.in_scale[i];
+    sc.in_offset[i] = -m.in_shift[i] * m.in_scale[i];
   }
 }
 
@@ -90,6 +119,7 @@ int launch(psl_grid* g) {
   p.rx.cs18 = 18.f * g->cs;
   p.mlp = &static_cast<const MlpBoth*>(g->mlp)->cta;
   p.mlpw = &static_cast<const MlpBoth*>(g->mlp)->warp;
+  std::memcpy(&p.sc, g->mlp_scalars, sizeof(MlpScalars));
   p.nu = g->info.nu;
   p.width = g->mlp_width;
   p.n = g->n;
@@ -137,8 +167,9 @@ int psl_set_sgs_mlp(psl_grid* g, const psl_sgs_mlp* mlp, float filter_width) {
   }
   if (g->storage == kStoreF64) return fail(PSL_ERR_INVALID, "psl_set_sgs_mlp: FP64 storage is for oracle runs only");
   MlpBoth host;
+  MlpScalars sc;
   pack(*mlp, host.cta);
-  pack_warp(*mlp, host.warp);
+  pack_warp(*mlp, host.warp, sc);
   if (!g->mlp) {
     cudaError_t e = cudaMalloc(&g->mlp, sizeof(MlpBoth));
     if (e != cudaSuccess) {
@@ -150,6 +181,7 @@ int psl_set_sgs_mlp(psl_grid* g, const psl_sgs_mlp* mlp, float filter_width) {
   MLP_CUDA(cudaMemcpyAsync(g->mlp, &host, sizeof(MlpBoth), cudaMemcpyHostToDevice, g->stream));
   MLP_CUDA(cudaStreamSynchronize(g->stream));
   g->mlp_width = filter_width;
+  std::memcpy(g->mlp_scalars, &sc, sizeof(MlpScalars));
   return PSL_OK;
 }
 

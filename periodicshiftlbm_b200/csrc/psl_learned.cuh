@@ -11,8 +11,9 @@
 // Two evaluations of the closure, one kernel each (same arithmetic around them):
 //   step_learned_warp_kernel  per-warp tensor-core MMAs (psl_mlp_warp.cuh), the default;
 //   step_learned_kernel       CTA-wide tcgen05 MMAs with TMEM accumulators (psl_mlp.cuh).
-// Both run one 128-cell tile per CTA and stage the weights (4-5 KB, from L2) per CTA (the
-// tcgen05 kernel also allocates and frees its 32 TMEM columns per CTA): a persistent loop
+// Both run one 128-cell tile per CTA (the tcgen05 kernel stages its weights in shared memory
+// and allocates and frees its 32 TMEM columns per CTA; the per-warp kernel reads its weights
+// from global memory in fragment order, without a CTA barrier): a persistent loop
 // over tiles made the compiler keep the 54 row offsets of the RowIndex in registers across
 // iterations (120 registers against 72 for one tile per CTA).  Every thread takes part in
 // its tile's MMAs (skip, solid and out-of-range cells with zero features), so the warp- or
@@ -32,7 +33,8 @@ struct LearnedParams {
   float4 given_uniform;
   RelaxationT<float> rx;    // Smagorinsky fallback
   const MlpDevice* mlp;      // tcgen05 layout
-  const MlpWarp* mlpw;       // per-warp layout
+  const MlpFrag* mlpw;       // per-warp layout (fragment order, global memory)
+  MlpScalars sc;             // normalisation, b3, output scale of the per-warp path
   float nu;                 // lattice viscosity of the grid
   float width;              // filter width fed to the closure (cell size / coarsest cell size)
   uint32_t n;
@@ -84,15 +86,7 @@ __global__ void __launch_bounds__(kMlpRows) step_learned_kernel(const __grid_con
 
 template <typename S>
 __global__ void __launch_bounds__(kStepThreads, 7) step_learned_warp_kernel(const __grid_constant__ LearnedParams<S> p) {
-  __shared__ MlpWarp w;
   __shared__ __align__(16) __half xtile[kStepThreads / 32][32 * kXStride];
-  {
-    const int4* src = reinterpret_cast<const int4*>(p.mlpw);
-    int4* dst = reinterpret_cast<int4*>(&w);
-    for (int i = threadIdx.x; i < (int)(sizeof(MlpWarp) / 16); i += blockDim.x) dst[i] = src[i];
-  }
-  // (the barrier that publishes the weights comes after the cell's loads and moments, so the
-  // weight copy overlaps them)
   __half* xt = xtile[threadIdx.x >> 5];
   {
     const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
@@ -118,8 +112,7 @@ __global__ void __launch_bounds__(kStepThreads, 7) step_learned_warp_kernel(cons
         mlp_features(K[2][0][0], K[0][2][0], K[0][0][2], K[1][1][0], K[1][0][1], K[0][1][1], rho, inv_rho, p.width, x);
       }
     }
-    __syncthreads();  // weights in shared memory; reached by every thread of the CTA
-    const float nu_t = mlp_warp_eval(w, xt, x);
+    const float nu_t = mlp_warp_eval(p.mlpw, p.sc, xt, x);  // converges the warp first
     if (kind != kSkip && kind != kSolid) {
       relax_rebuild(f, K, rho, ux, uy, uz, inv_rho, 1.f / (3.f * (p.nu + nu_t) + 0.5f));
       if (p.health) {

@@ -22,9 +22,10 @@
 //   layer 3: 2 x 2 MMAs (N = 8, row 0 of W3 holds the output weights)
 //   the output of row r sits in lane 4 (r % 8) (accumulator column 0); four shuffles bring
 //   it to lane r, the lane that owns the cell.
-// Weights live in shared memory as W[out][in] rows (ldmatrix of W rows yields the
-// column-major B fragments), rows padded to 48 / 80 bytes so the eight rows of an 8x8
-// ldmatrix read fall in distinct banks.
+// Weights stay in global memory (3.5 KB, L1-resident after the first warps), stored in
+// fragment order: each lane reads its own B fragments of an N-tile pair with one 16-byte
+// load, so no block copies them into shared memory and no block barrier waits for that copy.
+// The normalisation, b3 and the output scale are kernel parameters (constant-bank operands).
 #pragma once
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -34,22 +35,25 @@
 
 namespace psl {
 
-constexpr int kW1Stride = 24;  // halves per W1 row (16 used)
-constexpr int kW2Stride = 40;  // halves per W2 / W3 row (32 used)
 constexpr int kXStride = 24;   // halves per feature row of a warp's tile (16 used)
 
-struct MlpWarp {
-  __half w1[32 * kW1Stride];  // 1536 B
-  __half w2[32 * kW2Stride];  // 2560 B
-  __half w3[8 * kW2Stride];   //  640 B
-  float b2[32];           // layer-1 biases ride in W1 column 10 (input 10 is the constant 1)
-  float b3;
-  float out_scale;
+// B fragments of mma.m16n8k16 (.col B = W^T, B[k][n] = W[n][k]): lane l = 4 g + t holds,
+// for N-tile nt and K-step kk, b0 = (W[8nt+g][16kk+2t], W[8nt+g][16kk+2t+1]) and
+// b1 = (W[8nt+g][16kk+8+2t], W[8nt+g][16kk+9+2t]), FP16 pairs, lower column in the low half.
+struct MlpFrag {
+  uint4 w1[2][32];     // [np][lane]: {b0, b1} of N-tile 2np, {b0, b1} of N-tile 2np+1; K = 16
+                       // (inputs 0-9, input 10 the constant 1 times b1, 11-15 zero)
+  uint4 w2[2][2][32];  // [kk][np][lane]
+  uint4 w3[32];        // [lane]: {b0, b1} of K-step 0, {b0, b1} of K-step 1; row 0 = w3, rows 1-7 zero
+  float4 b2[2][32];    // [kk][lane]: b2 at columns 16kk+2t, 16kk+2t+1, 16kk+8+2t, 16kk+9+2t
+};
+
+struct MlpScalars {
   float in_scale[kMlpIn];  // normalised feature = x * in_scale + in_offset
   float in_offset[kMlpIn];
-  float pad[2];
+  float b3;
+  float out_scale;
 };
-static_assert(sizeof(MlpWarp) % 16 == 0, "MlpWarp is copied in 16-byte units");
 
 __device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
   asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
@@ -80,31 +84,27 @@ __device__ __forceinline__ uint32_t pack_relu(float a, float b) {
 }
 
 // (bias +) ReLU of the accumulators of N-tiles 2kk and 2kk+1 (columns 16kk..16kk+15) into
-// the A fragment of K-step kk of the next layer.
+// the A fragment of K-step kk of the next layer; bias = this lane's (b[c], b[c+1], b[c+8],
+// b[c+9]) for c = 16kk + 2t.
 template <bool kBias>
-__device__ __forceinline__ void acc_to_a(const float (&c0)[4], const float (&c1)[4], const float* bias, int col0,
-                                         uint32_t (&a)[4]) {
-  float2 bA = make_float2(0.f, 0.f), bB = make_float2(0.f, 0.f);
-  if (kBias) {
-    bA = *reinterpret_cast<const float2*>(bias + col0);
-    bB = *reinterpret_cast<const float2*>(bias + col0 + 8);
-  }
-  a[0] = pack_relu(c0[0] + bA.x, c0[1] + bA.y);
-  a[1] = pack_relu(c0[2] + bA.x, c0[3] + bA.y);
-  a[2] = pack_relu(c1[0] + bB.x, c1[1] + bB.y);
-  a[3] = pack_relu(c1[2] + bB.x, c1[3] + bB.y);
+__device__ __forceinline__ void acc_to_a(const float (&c0)[4], const float (&c1)[4], float4 bias, uint32_t (&a)[4]) {
+  if (!kBias) bias = make_float4(0.f, 0.f, 0.f, 0.f);
+  a[0] = pack_relu(c0[0] + bias.x, c0[1] + bias.y);
+  a[1] = pack_relu(c0[2] + bias.x, c0[3] + bias.y);
+  a[2] = pack_relu(c1[0] + bias.z, c1[1] + bias.w);
+  a[3] = pack_relu(c1[2] + bias.z, c1[3] + bias.w);
 }
 
 // nu_t of this lane's cell.  All 32 lanes of the warp must call it (converged); `xtile`
 // is the warp's 32 x kXStride FP16 staging tile in shared memory (16-byte aligned).
-__device__ __forceinline__ float mlp_warp_eval(const MlpWarp& w, __half* xtile, const float (&x)[kMlpIn]) {
+__device__ __forceinline__ float mlp_warp_eval(const MlpFrag* __restrict__ w, const MlpScalars& sc, __half* xtile,
+                                               const float (&x)[kMlpIn]) {
   const int lane = threadIdx.x & 31;
-  const int g = lane >> 2, t = lane & 3;
   // normalised features -> FP16 row `lane` (K padded to 16 with zeros)
   {
     float xn[16];
 #pragma unroll
-    for (int i = 0; i < kMlpIn; ++i) xn[i] = fmaf(x[i], w.in_scale[i], w.in_offset[i]);
+    for (int i = 0; i < kMlpIn; ++i) xn[i] = fmaf(x[i], sc.in_scale[i], sc.in_offset[i]);
     xn[kMlpIn] = 1.f;  // carries the layer-1 biases (W1 column 10)
 #pragma unroll
     for (int i = kMlpIn + 1; i < 16; ++i) xn[i] = 0.f;
@@ -121,10 +121,7 @@ __device__ __forceinline__ float mlp_warp_eval(const MlpWarp& w, __half* xtile, 
   __syncwarp();
   const int m = lane >> 3, r = lane & 7;  // ldmatrix: this lane addresses row r of matrix m
   const uint32_t xs = mlp_smem_u32(xtile);
-  const uint32_t w1s = mlp_smem_u32(w.w1), w2s = mlp_smem_u32(w.w2), w3s = mlp_smem_u32(w.w3);
-  // B fragments of W3 for both K-steps: matrices (k 0-7, 8-15, 16-23, 24-31) of rows 0-7
-  uint32_t b3[4];
-  ldsm_x4(w3s + (r * kW2Stride + 8 * m) * 2, b3[0], b3[1], b3[2], b3[3]);
+  const uint4 b3 = __ldg(&w->w3[lane]);  // W3's fragments for both K-steps
   float z[2][4];
 #pragma unroll
   for (int mt = 0; mt < 2; ++mt) {
@@ -134,47 +131,44 @@ __device__ __forceinline__ float mlp_warp_eval(const MlpWarp& w, __half* xtile, 
     float c1[4][4];
 #pragma unroll
     for (int np = 0; np < 2; ++np) {
-      uint32_t b[4];
-      ldsm_x4(w1s + ((8 * (2 * np + (m >> 1)) + r) * kW1Stride + 8 * (m & 1)) * 2, b[0], b[1], b[2], b[3]);
-      mma16816_new(c1[2 * np], a[0], a[1], a[2], a[3], b[0], b[1]);
-      mma16816_new(c1[2 * np + 1], a[0], a[1], a[2], a[3], b[2], b[3]);
+      const uint4 b = __ldg(&w->w1[np][lane]);
+      mma16816_new(c1[2 * np], a[0], a[1], a[2], a[3], b.x, b.y);
+      mma16816_new(c1[2 * np + 1], a[0], a[1], a[2], a[3], b.z, b.w);
     }
     uint32_t a2[2][4];
-    acc_to_a<false>(c1[0], c1[1], nullptr, 0, a2[0]);
-    acc_to_a<false>(c1[2], c1[3], nullptr, 0, a2[1]);
+    acc_to_a<false>(c1[0], c1[1], make_float4(0.f, 0.f, 0.f, 0.f), a2[0]);
+    acc_to_a<false>(c1[2], c1[3], make_float4(0.f, 0.f, 0.f, 0.f), a2[1]);
     // ---- layer 2 ----
     float c2[4][4];
 #pragma unroll
     for (int kk = 0; kk < 2; ++kk)
 #pragma unroll
       for (int np = 0; np < 2; ++np) {
-        uint32_t b[4];
-        ldsm_x4(w2s + ((8 * (2 * np + (m >> 1)) + r) * kW2Stride + 16 * kk + 8 * (m & 1)) * 2, b[0], b[1], b[2], b[3]);
+        const uint4 b = __ldg(&w->w2[kk][np][lane]);
         if (kk == 0) {
-          mma16816_new(c2[2 * np], a2[0][0], a2[0][1], a2[0][2], a2[0][3], b[0], b[1]);
-          mma16816_new(c2[2 * np + 1], a2[0][0], a2[0][1], a2[0][2], a2[0][3], b[2], b[3]);
+          mma16816_new(c2[2 * np], a2[0][0], a2[0][1], a2[0][2], a2[0][3], b.x, b.y);
+          mma16816_new(c2[2 * np + 1], a2[0][0], a2[0][1], a2[0][2], a2[0][3], b.z, b.w);
         } else {
-          mma16816(c2[2 * np], a2[1][0], a2[1][1], a2[1][2], a2[1][3], b[0], b[1]);
-          mma16816(c2[2 * np + 1], a2[1][0], a2[1][1], a2[1][2], a2[1][3], b[2], b[3]);
+          mma16816(c2[2 * np], a2[1][0], a2[1][1], a2[1][2], a2[1][3], b.x, b.y);
+          mma16816(c2[2 * np + 1], a2[1][0], a2[1][1], a2[1][2], a2[1][3], b.z, b.w);
         }
       }
     uint32_t a3[2][4];
-    acc_to_a<true>(c2[0], c2[1], w.b2, 2 * t, a3[0]);
-    acc_to_a<true>(c2[2], c2[3], w.b2, 16 + 2 * t, a3[1]);
+    acc_to_a<true>(c2[0], c2[1], __ldg(&w->b2[0][lane]), a3[0]);
+    acc_to_a<true>(c2[2], c2[3], __ldg(&w->b2[1][lane]), a3[1]);
     // ---- layer 3 (column 0 of the N = 8 tile) ----
-    mma16816_new(z[mt], a3[0][0], a3[0][1], a3[0][2], a3[0][3], b3[0], b3[1]);
-    mma16816(z[mt], a3[1][0], a3[1][1], a3[1][2], a3[1][3], b3[2], b3[3]);
+    mma16816_new(z[mt], a3[0][0], a3[0][1], a3[0][2], a3[0][3], b3.x, b3.y);
+    mma16816(z[mt], a3[1][0], a3[1][1], a3[1][2], a3[1][3], b3.z, b3.w);
   }
-  (void)g;
   // row rr of M-tile mt sits in lane 4 (rr % 8): register 0 for rr < 8, register 2 above
   const int src = 4 * (lane & 7);
   const float s00 = __shfl_sync(0xffffffffu, z[0][0], src);
   const float s02 = __shfl_sync(0xffffffffu, z[0][2], src);
   const float s10 = __shfl_sync(0xffffffffu, z[1][0], src);
   const float s12 = __shfl_sync(0xffffffffu, z[1][2], src);
-  const float zz = (lane < 8 ? s00 : lane < 16 ? s02 : lane < 24 ? s10 : s12) + w.b3;
+  const float zz = (lane < 8 ? s00 : lane < 16 ? s02 : lane < 24 ? s10 : s12) + sc.b3;
   const float sp = zz > 20.f ? zz : log1pf(__expf(zz));
-  return w.out_scale * sp;
+  return sc.out_scale * sp;
 }
 
 }  // namespace psl

@@ -144,6 +144,11 @@ int psl_apply_bc_periodic_x(psl_grid* grid);
 int psl_apply_bc_periodic_y(psl_grid* grid);
 /* applyCoarseFineGridCommunication (gridRefinementFunctions.h:433-526): one kernel. */
 int psl_apply_coarse_fine_grid_communication(psl_grid* coarse, psl_grid* fine);
+/* fillCoarseGridFromFine (gridRefinementFunctions.h:528-535): every coarse cell of
+ * [iS+1, iE-1) x [jS+1, jE-1) x [kS+1, kE-1) (inside the refinement block) becomes the
+ * rescaled average of its 8 fine children, as the reference does before exporting the coarse
+ * level.  Stream-ordered on the coarse grid's stream. */
+int psl_fill_coarse_grid_from_fine(psl_grid* coarse, psl_grid* fine);
 /* updateGrid recursion of the case driver (flowAroundSphereMainSingle.cu:158-167):
  * streaming + update on grids[level], two steps of level+1, coarse/fine transfer. */
 int psl_update_grid(psl_grid** grids, int levels, int level);

@@ -120,6 +120,9 @@ inline void applyBCPeriodicY(GridStruct& g) { check(psl_apply_bc_periodic_y(g.ha
 inline void applyCoarseFineGridCommunication(GridStruct& coarse, GridStruct& fine) {
   check(psl_apply_coarse_fine_grid_communication(coarse.handle(), fine.handle()), "applyCoarseFineGridCommunication");
 }
+inline void fillCoarseGridFromFine(GridStruct& coarse, GridStruct& fine) {
+  check(psl_fill_coarse_grid_from_fine(coarse.handle(), fine.handle()), "fillCoarseGridFromFine");
+}
 // fillEquilibriumFromFunction with the sphere case's start hook, or a uniform state.
 inline void fillEquilibriumFromFunction(GridStruct& g, const psl_sphere_case& sc) {
   check(psl_fill_equilibrium_sphere(g.handle(), &sc), "fillEquilibriumFromFunction");

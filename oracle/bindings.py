@@ -109,6 +109,7 @@ class _SimLib:
         getattr(L, p + "sim_get_shifts").argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         getattr(L, p + "sim_drag").restype = ctypes.c_double
         getattr(L, p + "sim_drag").argtypes = [ctypes.c_void_p]
+        getattr(L, p + "sim_fill_coarse_from_fine").argtypes = [ctypes.c_void_p, ctypes.c_int]
 
     def _fn(self, name):
         return getattr(self.lib, self.prefix + name)
@@ -158,6 +159,10 @@ class Sim:
 
     def drag(self) -> float:
         return float(self.owner._fn("sim_drag")(self.h))
+
+    def fill_coarse_from_fine(self, level: int = 0):
+        """fillCoarseGridFromFine on levels `level` and `level` + 1."""
+        self.owner._fn("sim_fill_coarse_from_fine")(self.h, int(level))
 
 
 class RefLib(_SimLib):

@@ -720,6 +720,20 @@ void oracle_sim_get_shifts(void* p, int level, int* out) {
   for (int q = 0; q < 27; ++q)
     out[q] = (int)(h->isDouble ? h->sd->grids[level].shift[q] : h->sf->grids[level].shift[q]);
 }
+// fillCoarseGridFromFine (gridRefinementFunctions.h:528-535): restriction of the coarse box
+// [iS+1, iE-1) x [jS+1, jE-1) x [kS+1, kE-1) of level `level` from level `level` + 1.
+void oracle_sim_fill_coarse_from_fine(void* p, int level) {
+  OracleHandle* h = static_cast<OracleHandle*>(p);
+  auto fill = [level](auto& sim) {
+    auto& gc = sim.grids[level];
+    auto& gf = sim.grids[level + 1];
+    const Info& C = gc.info;
+    const int b0[3] = {C.iS + 1, C.jS + 1, C.kS + 1}, b1[3] = {C.iE - 1, C.jE - 1, C.kE - 1};
+    restrictBox(gc, gf, b0, b1);
+  };
+  if (h->isDouble) fill(*h->sd);
+  else fill(*h->sf);
+}
 double oracle_sim_drag(void* p) {
   OracleHandle* h = static_cast<OracleHandle*>(p);
   return h->isDouble ? dragLattice(*h->sd) : dragLattice(*h->sf);

@@ -488,5 +488,9 @@ void ref_streaming(int nx, int ny, int nz, int* shifts27) {
 void ref_sim_periodic_x(void* h, int level) { applyBCPeriodicX(static_cast<RefSim*>(h)->grids[level]); }
 void ref_sim_periodic_y(void* h, int level) { applyBCPeriodicY(static_cast<RefSim*>(h)->grids[level]); }
 void ref_sim_streaming(void* h, int level) { applyStreaming(static_cast<RefSim*>(h)->grids[level]); }
+void ref_sim_fill_coarse_from_fine(void* h, int level) {
+  RefSim* s = static_cast<RefSim*>(h);
+  fillCoarseGridFromFine(s->grids[level], s->grids[level + 1]);
+}
 
 }  // extern "C"

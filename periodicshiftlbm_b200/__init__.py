@@ -11,6 +11,7 @@ from .grid import (  # noqa: F401
     applyBCPeriodicX,
     applyBCPeriodicY,
     applyCoarseFineGridCommunication,
+    fillCoarseGridFromFine,
     applyLocalCellUpdate,
     applyStreaming,
     debug_cells,

@@ -99,6 +99,7 @@ _SIGNATURES = {
     "psl_apply_bc_periodic_x": (ctypes.c_int, [ctypes.c_void_p]),
     "psl_apply_bc_periodic_y": (ctypes.c_int, [ctypes.c_void_p]),
     "psl_apply_coarse_fine_grid_communication": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "psl_fill_coarse_grid_from_fine": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_update_grid": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int]),
     "psl_sphere_force": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PslSphereCase), ctypes.c_void_p]),
     "psl_momentum_exchange_force_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p,

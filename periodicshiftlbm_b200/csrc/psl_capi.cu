@@ -619,6 +619,50 @@ static int launch_coarse_fine(psl_grid* c, psl_grid* f) {
   return PSL_OK;
 }
 
+// The geometry the restriction reads: both grids' rows, dimensions and the block bounds.
+template <typename S>
+static CoarseFineParams<S> block_params(psl_grid* c, psl_grid* f) {
+  CoarseFineParams<S> p{};
+  p.c = row_index<S>(c);
+  p.f = row_index<S>(f);
+  p.cnx = c->info.cell_count_x;
+  p.cny = c->info.cell_count_y;
+  p.cnz = c->info.cell_count_z;
+  p.iS = c->info.i_subgrid_start; p.jS = c->info.j_subgrid_start; p.kS = c->info.k_subgrid_start;
+  p.iE = c->info.i_subgrid_end; p.jE = c->info.j_subgrid_end; p.kE = c->info.k_subgrid_end;
+  p.fnx = f->info.cell_count_x;
+  p.fny = f->info.cell_count_y;
+  p.fnz = f->info.cell_count_z;
+  return p;
+}
+
+template <typename S>
+static int launch_fill_coarse(psl_grid* c, psl_grid* f) {
+  const CoarseFineParams<S> p = block_params<S>(c, f);
+  const uint32_t cells = (uint32_t)(p.iE - p.iS - 2) * (uint32_t)(p.jE - p.jS - 2) * (uint32_t)(p.kE - p.kS - 2);
+  fill_coarse_kernel<S><<<blocks_for(cells, kCoarseFineThreads), kCoarseFineThreads, 0, c->stream>>>(p);
+  PSL_CUDA(cudaGetLastError());
+  return PSL_OK;
+}
+
+int psl_fill_coarse_grid_from_fine(psl_grid* c, psl_grid* f) {
+  PSL_CHECK(c && f, PSL_ERR_INVALID, "psl_fill_coarse_grid_from_fine: null grid");
+  PSL_CHECK(c->storage == f->storage, PSL_ERR_INVALID,
+            "psl_fill_coarse_grid_from_fine: coarse and fine grids use different storage");
+  const psl_info& C = c->info;
+  const psl_info& F = f->info;
+  const int a = C.i_subgrid_end - C.i_subgrid_start, b = C.j_subgrid_end - C.j_subgrid_start,
+            cc = C.k_subgrid_end - C.k_subgrid_start;
+  PSL_CHECK(a >= 4 && b >= 4 && cc >= 4, PSL_ERR_INVALID, "fill coarse: refinement block needs >= 4 cells per axis");
+  PSL_CHECK(F.cell_count_x == 2 * a && F.cell_count_y == 2 * b && F.cell_count_z == 2 * cc, PSL_ERR_INVALID,
+            "fill coarse: fine grid is not twice the refinement block");
+  PSL_CHECK(c->device == f->device, PSL_ERR_INVALID, "fill coarse: grids on different devices");
+  PSL_CHECK(27ull * c->stride + c->n < (1ull << 32) && 27ull * f->stride + f->n < (1ull << 32), PSL_ERR_INVALID,
+            "fill coarse: grid too large for 32-bit row offsets");
+  DeviceGuard dg(c->device);
+  return with_storage(c->storage, [&](auto s) { return launch_fill_coarse<decltype(s)>(c, f); });
+}
+
 int psl_apply_coarse_fine_grid_communication(psl_grid* c, psl_grid* f) {
   PSL_CHECK(c && f, PSL_ERR_INVALID, "psl_apply_coarse_fine_grid_communication: null grid");
   PSL_CHECK(c->storage == f->storage, PSL_ERR_INVALID,

@@ -545,6 +545,46 @@ __device__ __forceinline__ void store_pop(const RowIndex<S>& r, int q, uint32_t 
 
 constexpr int kCoarseFineThreads = 128;
 
+// Coarse cell (i, j, k) of the refined block from its 8 fine children: their populations
+// added in the child order (k, j, i outer to inner), averaged, rescaled fine -> coarse
+// (writeToCoarseGridInterface, gridRefinementFunctions.h:283-336).
+template <typename S>
+__device__ __forceinline__ void restrict_cell(const RowIndex<S>& rc, const RowIndex<S>& rf, const CoarseFineParams<S>& p,
+                                              int i, int j, int k) {
+  using T = typename S::calc;
+  const int fi = (i - p.iS) * 2, fj = (j - p.jS) * 2, fk = (k - p.kS) * 2;
+  T f[27];
+#pragma unroll
+  for (int q = 0; q < 27; ++q) f[q] = T(0);
+#pragma unroll
+  for (int dk = 0; dk <= 1; ++dk)
+#pragma unroll
+    for (int dj = 0; dj <= 1; ++dj)
+#pragma unroll
+      for (int di = 0; di <= 1; ++di) {
+        const uint32_t fc = ((uint32_t)(fk + dk) * p.fny + (fj + dj)) * p.fnx + (fi + di);
+#pragma unroll
+        for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], load_pop(rf, q, fc));
+      }
+#pragma unroll
+  for (int q = 0; q < 27; ++q) f[q] = f[q] * T(0.125);
+  rescale(f, false);
+  const uint32_t cc = ((uint32_t)k * p.cny + j) * p.cnx + i;
+#pragma unroll
+  for (int q = 0; q < 27; ++q) store_pop(rc, q, cc, f[q]);
+}
+
+// fillCoarseGridFromFine (gridRefinementFunctions.h:528-535): every coarse cell of the box
+// [iS+1, iE-1) x [jS+1, jE-1) x [kS+1, kE-1) -- the refined region inside the ring, ring
+// included -- restricted from the fine grid (one thread per coarse cell, i fastest).
+template <typename S>
+__global__ void __launch_bounds__(kCoarseFineThreads) fill_coarse_kernel(const __grid_constant__ CoarseFineParams<S> p) {
+  const uint32_t a = p.iE - p.iS - 2, b = p.jE - p.jS - 2, c = p.kE - p.kS - 2;
+  const uint32_t t = blockIdx.x * kCoarseFineThreads + threadIdx.x;
+  if (t >= a * b * c) return;
+  restrict_cell(p.c, p.f, p, p.iS + 1 + (int)(t % a), p.jS + 1 + (int)((t / a) % b), p.kS + 1 + (int)(t / (a * b)));
+}
+
 template <typename S>
 __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const __grid_constant__ CoarseFineParams<S> p) {
   using T = typename S::calc;
@@ -587,27 +627,7 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
         rj = 1 + r % (b - 2);
         rk = 1 + r / (b - 2);
       }
-      const int i = p.iS + 1 + ri, j = p.jS + 1 + rj, k = p.kS + 1 + rk;
-      const int fi = (i - p.iS) * 2, fj = (j - p.jS) * 2, fk = (k - p.kS) * 2;
-      T f[27];
-#pragma unroll
-      for (int q = 0; q < 27; ++q) f[q] = T(0);
-#pragma unroll
-      for (int dk = 0; dk <= 1; ++dk)
-#pragma unroll
-        for (int dj = 0; dj <= 1; ++dj)
-#pragma unroll
-          for (int di = 0; di <= 1; ++di) {
-            const uint32_t fc = ((uint32_t)(fk + dk) * p.fny + (fj + dj)) * p.fnx + (fi + di);
-#pragma unroll
-            for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], load_pop(rf, q, fc));
-          }
-#pragma unroll
-      for (int q = 0; q < 27; ++q) f[q] = f[q] * T(0.125);
-      rescale(f, false);
-      const uint32_t cc = ((uint32_t)k * p.cny + j) * p.cnx + i;
-#pragma unroll
-      for (int q = 0; q < 27; ++q) store_pop(rc, q, cc, f[q]);
+      restrict_cell(rc, rf, p, p.iS + 1 + ri, p.jS + 1 + rj, p.kS + 1 + rk);
     }
   }
   grid_barrier(p.barrier, p.nblocks, p.error);

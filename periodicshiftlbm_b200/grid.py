@@ -289,6 +289,13 @@ def applyCoarseFineGridCommunication(coarse: GridStruct, fine: GridStruct):
     call("psl_apply_coarse_fine_grid_communication", coarse.handle, fine.handle)
 
 
+def fillCoarseGridFromFine(coarse: GridStruct, fine: GridStruct):
+    """gridRefinementFunctions.h:528-535: the coarse cells inside the refinement block take
+    the rescaled average of their fine children (the reference calls it before exporting the
+    coarse level)."""
+    call("psl_fill_coarse_grid_from_fine", coarse.handle, fine.handle)
+
+
 def updateGrid(grids, level: int = 0):
     """The driver's updateGrid recursion (flowAroundSphereMainSingle.cu:158-167), run in
     the library so one call issues a whole coarse step."""

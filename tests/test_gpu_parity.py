@@ -177,3 +177,29 @@ def test_config2_full_size_matches_reference(ref):
         del fg, fr
     assert abs(sim.drag() - r.drag()) <= 1e-4 * abs(r.drag())
     sim.close()
+
+
+def test_fill_coarse_from_fine_matches_reference(ref):
+    """psl_fill_coarse_grid_from_fine against the reference's fillCoarseGridFromFine after the
+    same 2-level run: the coarse level within FP32 rounding, cells outside the block and the
+    fine level untouched."""
+    from periodicshiftlbm_b200 import fillCoarseGridFromFine
+
+    c = CASES["small_refined_les"]
+    sim, r = GpuSim(c), ref.sim(c)
+    sim.run(6)
+    r.run(6)
+    before_c, before_f = sim.populations(0), sim.populations(1)
+    fillCoarseGridFromFine(sim.grids[0], sim.grids[1])
+    r.fill_coarse_from_fine(0)
+    fg = sim.populations(0)
+    (i0, j0, k0), (i1, j1, k1) = c.refine
+    inside = np.zeros((c.nz, c.ny, c.nx), dtype=bool)
+    inside[k0 + 1:k1 - 1, j0 + 1:j1 - 1, i0 + 1:i1 - 1] = True
+    inside = inside.ravel()
+    assert rel(fg, r.populations(0)) < 1e-5
+    assert np.array_equal(fg[:, ~inside], before_c[:, ~inside])
+    assert not np.array_equal(fg[:, inside], before_c[:, inside])
+    assert np.array_equal(sim.populations(1), before_f)
+    assert sim.grids[0].health() == 0
+    sim.close()

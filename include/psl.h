@@ -150,7 +150,11 @@ int psl_apply_coarse_fine_grid_communication(psl_grid* coarse, psl_grid* fine);
  * level.  Stream-ordered on the coarse grid's stream. */
 int psl_fill_coarse_grid_from_fine(psl_grid* coarse, psl_grid* fine);
 /* updateGrid recursion of the case driver (flowAroundSphereMainSingle.cu:158-167):
- * streaming + update on grids[level], two steps of level+1, coarse/fine transfer. */
+ * streaming + update on grids[level], two steps of level+1, coarse/fine transfer.
+ * Kernels go to each grid's stream in call order.  The periodic shifts are kernel
+ * parameters taken when the update is launched, so a step recorded by stream capture replays
+ * with that step's shifts: for replaying steps from a CUDA graph use psl_batch_*, whose
+ * kernels derive the shifts from a step counter on the device. */
 int psl_update_grid(psl_grid** grids, int levels, int level);
 
 /* ---- reductions (FP64) ---- */

@@ -1,8 +1,8 @@
 // C ABI of the batched update (include/psl.h, "batched form"): a batch of independent
-// single-level grids advanced by one persistent kernel per step (psl_batch.cuh), the step
-// captured once in a CUDA graph and replayed, and a project-written autotuner that picks
-// the launch shape (threads per CTA, cells per tile, resident CTAs per SM) by timing
-// candidates on the batch itself.
+// single-level grids advanced by one kernel per step over all their tiles (psl_batch.cuh),
+// the step captured once in a CUDA graph and replayed, and a project-written autotuner that
+// picks the launch shape (threads per CTA, cells per warp tile, resident CTAs per SM or a
+// one-pass grid) by timing candidates on the batch itself.
 #include <cuda_runtime.h>
 
 #include <algorithm>

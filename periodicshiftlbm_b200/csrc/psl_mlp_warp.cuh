@@ -22,7 +22,7 @@
 //   layer 3: 2 x 2 MMAs (N = 8, row 0 of W3 holds the output weights)
 //   the output of row r sits in lane 4 (r % 8) (accumulator column 0); four shuffles bring
 //   it to lane r, the lane that owns the cell.
-// Weights stay in global memory (3.5 KB, L1-resident after the first warps), stored in
+// Weights stay in global memory (4.6 KB with the biases, L1-resident after the first warps), stored in
 // fragment order: each lane reads its own B fragments of an N-tile pair with one 16-byte
 // load, so no block copies them into shared memory and no block barrier waits for that copy.
 // The normalisation, b3 and the output scale are kernel parameters (constant-bank operands).

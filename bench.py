@@ -17,7 +17,10 @@ persistent kernel per step from a captured CUDA graph, launch shape from the aut
 Prints ONE JSON line (rank 0).  `value` is MLUPS over the device-timed region (CUDA events,
 max over ranks); `e2e` is the same metric through the public API with host buffers: the
 state is uploaded from pinned host memory, every step reads the FP64 drag back to the host
-(as the reference driver does), and the final state is downloaded.
+(as the reference driver does), and the final state is downloaded.  The default FP32 plain
+run also measures the metric's second form on the same case and step counts --
+`forms.f16_mlp`: FP16 f - w storage with the learned closure -- with its roofline, its
+speed-up over the plain form and its drag beside the plain form's (`--no-forms` skips it).
 """
 from __future__ import annotations
 
@@ -55,6 +58,8 @@ def parse():
     p.add_argument("--batch-cases", type=int, default=64)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-steps", type=int, default=2)
+    p.add_argument("--no-forms", dest="forms", action="store_false",
+                   help="only the selected form (default: FP32 plain also measures FP16 + learned closure)")
     return p.parse_args()
 
 
@@ -167,12 +172,10 @@ def hbm_peak():
         return 6650.0, "fallback"
 
 
-def closure_kernel() -> tuple:
-    """(kernel name, label) of the learned-closure update the library runs: the per-warp
-    MMA kernel unless PSL_CLOSURE_PATH=tcgen05 selects the CTA-wide tcgen05 one."""
-    if os.environ.get("PSL_CLOSURE_PATH") == "tcgen05":
-        return "step_learned_kernel", "tcgen05, CTA-wide"
-    return "step_learned_warp_kernel", "per-warp MMA"
+def update_kernel(storage: str, sgs: str) -> str:
+    """The coarse-grid update kernel the library launches for this form: the pipelined tile
+    kernels (the config-2 grids hold a multiple of 16 bytes of elements)."""
+    return "step_pipe_learned_kernel" if sgs == "mlp" else "step_pipe_kernel"
 
 
 def batch_traffic(storage: str, cells: int):
@@ -186,8 +189,8 @@ def batch_traffic(storage: str, cells: int):
 
 
 def ncu_traffic(kernel: str, storage: str):
-    """dram bytes read+written per launch of the coarse update kernel from the committed
-    ncu summary (profiles/<kernel>_<storage>_sphere512.md), or None."""
+    """DRAM bytes read + written by one coarse-grid launch of `kernel`, from the committed
+    ncu summary profiles/<kernel>_<storage>_sphere512.md (a full-size capture), or None."""
     path = os.path.join(REPO, "profiles", f"{kernel}_{storage}_sphere512.md")
     if not os.path.exists(path):
         return None
@@ -198,17 +201,11 @@ def ncu_traffic(kernel: str, storage: str):
 # ------------------------------------------------------------------------------------------
 # native (CUDA) arm
 # ------------------------------------------------------------------------------------------
-def run_native(args):
+def measure_form(args, cfg, storage: str, sgs: str, world: int, local: int, with_e2e: bool) -> dict:
+    """One form of the update on config `cfg`: W warm-up steps, K device-timed steps (CUDA
+    events on the grids' stream, max over ranks), the drag after those W + K steps, and
+    (with_e2e) K more steps end to end through the public API with host buffers."""
     import torch
-
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     from periodicshiftlbm_b200 import (
         applyCoarseFineGridCommunication,
@@ -218,12 +215,11 @@ def run_native(args):
     )
     from periodicshiftlbm_b200.cases import make_sphere_grids
 
-    cfg = workload(args)
     stream = torch.cuda.Stream()
-    grids, case = make_sphere_grids(cfg, storage=args.storage)
+    grids, case = make_sphere_grids(cfg, storage=storage)
     for g in grids:
         g.set_stream(stream.cuda_stream)
-    if args.sgs == "mlp":
+    if sgs == "mlp":
         from periodicshiftlbm_b200.sgs import load_params, set_sgs_mlp
 
         closure = load_params()
@@ -273,102 +269,142 @@ def run_native(args):
     barrier()
     ms = max_over_ranks(t0.elapsed_time(t1), world)
     updates = cfg.updates_per_step()
-    value = job_rate(updates, args.steps, world, ms)
-
+    drag_after = float(getSphereForce(grids[-1], case)[0])
+    out = {
+        "storage": storage, "sgs": sgs, "updates": updates, "ms": ms, "levels": levels, "clocks": clocks,
+        "value": job_rate(updates, args.steps, world, ms), "drag_after_timed": drag_after,
+        "coarse_ms": statistics.mean(a.elapsed_time(b) for a, b in ev["coarse"]),
+        "fine_ms": statistics.mean(a.elapsed_time(b) for a, b in ev["fine"]) if ev["fine"] else None,
+    }
     # roofline of the dominant kernel: the coarse-grid update
-    coarse_ms = statistics.mean(a.elapsed_time(b) for a, b in ev["coarse"])
-    fine_ms = statistics.mean(a.elapsed_time(b) for a, b in ev["fine"]) if ev["fine"] else None
     info0 = cfg.infos()[0]
     coarse_updates = info0.cellCount
     if cfg.refine:
         (i0, j0, k0), (i1, j1, k1) = cfg.refine
         coarse_updates -= (i1 - i0 - 4) * (j1 - j0 - 4) * (k1 - k0 - 4)
-    bpu = BYTES_PER_UPDATE[args.storage]
-    coarse_bytes = bpu * coarse_updates
+    bpu = BYTES_PER_UPDATE[storage]
     peak, peak_kind = hbm_peak()
-    achieved = coarse_bytes / (coarse_ms * 1e-3) / 1e9
-
-    # ---- end to end through the public API with host buffers ----
-    pinned_in = [torch.empty((27, g.cellCount), dtype=torch.float32).pin_memory() for g in grids]
-    pinned_out = [torch.empty((27, g.cellCount), dtype=torch.float32).pin_memory() for g in grids]
-    for g, h in zip(grids, pinned_in):
-        g.read_populations(h.numpy())
-    host_state = [h.numpy() for h in pinned_in]
+    achieved = bpu * coarse_updates / (out["coarse_ms"] * 1e-3) / 1e9
+    kernel = update_kernel(storage, sgs)
+    out["roofline"] = {
+        "bound": "hbm", "kernel": kernel + " (coarse grid)", "achieved": round(achieved, 1), "peak": peak,
+        "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+        "traffic": ncu_traffic(kernel, storage), "algorithmic_bytes_per_launch": bpu * coarse_updates,
+        "launch_ms": round(out["coarse_ms"], 4),
+        "fine_launch_ms": round(out["fine_ms"], 4) if out["fine_ms"] else None,
+        "whole_step_frac": round(bpu * updates / (ms / args.steps * 1e-3) / 1e9 / peak, 4),
+    }
+    if with_e2e:
+        # ---- end to end through the public API with host buffers ----
+        pinned_in = [torch.empty((27, g.cellCount), dtype=torch.float32).pin_memory() for g in grids]
+        pinned_out = [torch.empty((27, g.cellCount), dtype=torch.float32).pin_memory() for g in grids]
+        for g, h in zip(grids, pinned_in):
+            g.read_populations(h.numpy())
+        torch.cuda.synchronize()
+        barrier()
+        e0 = time.perf_counter()
+        for g, h in zip(grids, pinned_in):
+            g.write_populations(h.numpy())
+        drags = []
+        for _ in range(args.steps):
+            update(0, False)
+            drags.append(float(getSphereForce(grids[-1], case)[0]))
+        for g, h in zip(grids, pinned_out):
+            g.read_populations(h.numpy())
+        torch.cuda.synchronize()
+        e_s = max_over_ranks(time.perf_counter() - e0, world)
+        state_bytes = sum(h.numpy().nbytes for h in pinned_in)
+        out["e2e"] = {
+            "value": round(job_rate(updates, args.steps, world, e_s * 1e3), 1),
+            "unit": "MLUPS",
+            "h2d_bytes_per_step": round(state_bytes / args.steps),
+            "d2h_bytes_per_step": round(state_bytes / args.steps) + 24,
+            "note": "state uploaded once and downloaded once per run, drag read back every step",
+        }
+        out["drag_last"] = drags[-1] if drags else None
+    for g in grids:
+        g.close()
     torch.cuda.synchronize()
-    barrier()
-    e0 = time.perf_counter()
-    for g, h in zip(grids, pinned_in):
-        g.write_populations(h.numpy())
-    drags = []
-    for _ in range(args.steps):
-        update(0, False)
-        drags.append(float(getSphereForce(grids[-1], case)[0]))
-    for g, h in zip(grids, pinned_out):
-        g.read_populations(h.numpy())
-    torch.cuda.synchronize()
-    e_s = max_over_ranks(time.perf_counter() - e0, world)
-    state_bytes = sum(h.nbytes for h in host_state)
-    e2e_value = job_rate(updates, args.steps, world, e_s * 1e3)
+    return out
 
+
+def run_native(args):
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    cfg = workload(args)
+    main = measure_form(args, cfg, args.storage, args.sgs, world, local, with_e2e=True)
+    levels = main["levels"]
     line = {
         "metric": METRIC,
-        "value": round(value, 1),
+        "value": round(main["value"], 1),
         "unit": "MLUPS",
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": round(ms / args.steps, 4),
+        "ms_per_step": round(main["ms"] / args.steps, 4),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32" if args.storage == "f32" else f"{args.storage}-storage/f32-math",
         "data": "synthetic",
-        "config": {
-            "workload": cfg.name,
-            "grid": [cfg.nx, cfg.ny, cfg.nz],
-            "refine_block": cfg.refine,
-            "storage": args.storage,
-            "updates_per_step": updates,
-            "reference_formula_updates_per_step": cfg.reference_updates_per_step(),
-            "collision": (f"cumulant + learned MLP closure ({closure_kernel()[1]})" if args.sgs == "mlp" else
-                          "cumulant + Smagorinsky" if cfg.smagorinsky else "cumulant"),
-            "l2": "inputs larger than L2 (no flush)" if cfg.refine else "state fits partly in L2",
-            "parallelism": f"replicas x{world}",
-        },
-        "roofline": {
-            "bound": "hbm",
-            "kernel": (closure_kernel()[0] if args.sgs == "mlp" else "step_kernel") + " (coarse grid)",
-            "achieved": round(achieved, 1),
-            "peak": peak,
-            "peak_kind": peak_kind,
-            "unit": "GB/s",
-            "frac": round(achieved / peak, 4),
-            "traffic": ncu_traffic(closure_kernel()[0] if args.sgs == "mlp" else "step_kernel", args.storage),
-            "algorithmic_bytes_per_launch": coarse_bytes,
-            "launch_ms": round(coarse_ms, 4),
-            "fine_launch_ms": round(fine_ms, 4) if fine_ms else None,
-        },
-        "e2e": {
-            "value": round(e2e_value, 1),
-            "unit": "MLUPS",
-            "h2d_bytes_per_step": round(state_bytes / args.steps),
-            "d2h_bytes_per_step": round(state_bytes / args.steps) + 24,
-            "note": "state uploaded once and downloaded once per run, drag read back every step",
-        },
-        "gpu_launches": args.steps * (1 + 2 * (levels - 1) + (levels - 1)) if levels > 1 else args.steps,
-        "clocks": clocks,
-        "drag_last": drags[-1] if drags else None,
+        "config": config_dict(cfg, args.storage, args.sgs, world),
+        "roofline": main["roofline"],
+        "e2e": main["e2e"],
+        "gpu_launches": args.steps * (1 + 3 * (levels - 1)),
+        "clocks": main["clocks"],
+        "drag_after_timed": main["drag_after_timed"],
+        "drag_last": main.get("drag_last"),
     }
+    if args.forms and args.storage == "f32" and args.sgs == "smagorinsky":
+        # the metric's second form on the same case and step counts: FP16 f - w storage +
+        # the learned closure, against this FP32 plain run
+        alt = measure_form(args, cfg, "f16", "mlp", world, local, with_e2e=False)
+        plain_drag = main["drag_after_timed"]
+        line["forms"] = {
+            "f32_plain": {"value": round(main["value"], 1), "ms_per_step": round(main["ms"] / args.steps, 4),
+                          "roofline_frac": main["roofline"]["frac"],
+                          "whole_step_frac": main["roofline"]["whole_step_frac"],
+                          "drag_after_timed": plain_drag},
+            "f16_mlp": {"value": round(alt["value"], 1), "ms_per_step": round(alt["ms"] / args.steps, 4),
+                        "speedup_vs_f32_plain": round(alt["value"] / main["value"], 3),
+                        "roofline": alt["roofline"], "clocks": alt["clocks"],
+                        "drag_after_timed": alt["drag_after_timed"],
+                        "drag_rel_vs_f32_plain": round(abs(alt["drag_after_timed"] - plain_drag) / abs(plain_drag), 5),
+                        "note": "drag after the same warm-up + timed steps from the same start state; the "
+                                "converged-drag comparison (long runs) is in the precision study"},
+        }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, args.cpu_sample_steps)
-    for g in grids:
-        g.close()
     if world > 1:
         import torch.distributed as dist
 
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def config_dict(cfg, storage: str, sgs: str, world: int) -> dict:
+    """The `config` of a bench line; the reference arm reports the same keys."""
+    return {
+        "workload": cfg.name,
+        "grid": [cfg.nx, cfg.ny, cfg.nz],
+        "refine_block": cfg.refine,
+        "storage": storage,
+        "updates_per_step": cfg.updates_per_step(),
+        "reference_formula_updates_per_step": cfg.reference_updates_per_step(),
+        "collision": ("cumulant + learned MLP closure (per-warp tensor-core MMAs)" if sgs == "mlp" else
+                      "cumulant + Smagorinsky" if cfg.smagorinsky else "cumulant"),
+        "l2": "inputs larger than L2 (no flush)" if cfg.refine else "state fits partly in L2",
+        "parallelism": f"replicas x{world}",
+    }
 
 
 # ------------------------------------------------------------------------------------------
@@ -430,8 +466,7 @@ def run_reference(args):
         "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": done,
         "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / max(done, 1), 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-        "config": {"workload": cfg.name, "grid": [cfg.nx, cfg.ny, cfg.nz], "refine_block": cfg.refine,
-                   "updates_per_step": cfg.updates_per_step(), "parallelism": "host cores"},
+        "config": config_dict(cfg, "f32", "smagorinsky", world),
         "cpu_baseline": {"value": round(value, 2), "unit": "MLUPS", "cores": os.cpu_count(), "kind": kind,
                          "sample": sample},
         "e2e": {"value": round(value, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

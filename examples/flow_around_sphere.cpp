@@ -1,11 +1,14 @@
 // A reference-style case driver on the C++ mirror (include/psl.hpp): the loop of
 // flowAroundSphere/flowAroundSphereMainSingle.cu:245-264 -- updateGrid, then the drag --
-// on the 512x256x256 sphere case with one 2:1 refinement level.
+// on the 512x256x256 sphere case with one 2:1 refinement level (every length times
+// `scale`, the Reynolds number kept, as periodicshiftlbm_b200.cases.config2(scale)).
 //
-//   g++ -O2 -std=c++17 -I include examples/flow_around_sphere.cpp \
+//   g++ -O2 -std=c++17 -I include examples/flow_around_sphere.cpp
 //       periodicshiftlbm_b200/libpsl_b200.so -Wl,-rpath,$PWD/periodicshiftlbm_b200 -o sphere
-//   ./sphere [steps]
+//   (one command line)
+//   ./sphere [steps] [scale]
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -14,9 +17,11 @@
 
 int main(int argc, char** argv) {
   const int steps = argc > 1 ? std::atoi(argv[1]) : 100;
+  const double scale = argc > 2 ? std::atof(argv[2]) : 1.0;
+  auto sc_len = [&](double v) { return (int)std::lround(v * scale); };
   psl_sphere_case sc{};
-  sc.sphere_x = sc.sphere_y = sc.sphere_z = 128.f;
-  sc.sphere_r = 24.f;
+  sc.sphere_x = sc.sphere_y = sc.sphere_z = (float)(128.0 * scale);
+  sc.sphere_r = (float)(24.0 * scale);
   sc.u_in = 0.05f;
   sc.rho_given = 1.f;
   sc.wall_mode = 0;
@@ -26,12 +31,12 @@ int main(int argc, char** argv) {
 
   std::vector<psl::GridStruct> grids(2);
   psl::InfoStruct c;
-  c.cellCountX = 512;
-  c.cellCountY = c.cellCountZ = 256;
-  c.nu = 0.05f * 48.f / 1e5f;
-  c.iSubgridStart = c.jSubgridStart = c.kSubgridStart = 80;
-  c.iSubgridEnd = 208;
-  c.jSubgridEnd = c.kSubgridEnd = 176;
+  c.cellCountX = sc_len(512);
+  c.cellCountY = c.cellCountZ = sc_len(256);
+  c.nu = (float)(0.05 * 48 * scale / 1e5);
+  c.iSubgridStart = c.jSubgridStart = c.kSubgridStart = sc_len(80);
+  c.iSubgridEnd = sc_len(208);
+  c.jSubgridEnd = c.kSubgridEnd = sc_len(176);
   psl::InfoStruct f;  // flowAroundSphereMainSingle.cu:185-215
   f.gridID = 1;
   f.res = c.res * 0.5f;
@@ -56,8 +61,13 @@ int main(int argc, char** argv) {
     drag = psl::getSphereDrag(grids[1], sc);
   }
   const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  const double updates = 512.0 * 256 * 256 - 124.0 * 92 * 92 + 2.0 * 254 * 190 * 190;
-  std::printf("steps %d  drag %.6g  MLUPS %.1f (with a drag read-back every step)\n", steps, drag,
+  // cells updated per coarse step: the coarse grid less its refined interior, twice the
+  // fine grid less its ghost layer (include/applyLocalCellUpdate.h:25-30)
+  const double updates = (double)c.cellCountX * c.cellCountY * c.cellCountZ -
+                         (double)(c.iSubgridEnd - c.iSubgridStart - 4) * (c.jSubgridEnd - c.jSubgridStart - 4) *
+                             (c.kSubgridEnd - c.kSubgridStart - 4) +
+                         2.0 * (f.cellCountX - 2) * (f.cellCountY - 2) * (f.cellCountZ - 2);
+  std::printf("steps %d  drag %.17g  MLUPS %.1f (with a drag read-back every step)\n", steps, drag,
               updates * steps / s / 1e6);
   return 0;
 }

@@ -97,6 +97,13 @@ int psl_set_given(psl_grid* grid, float rho, float ux, float uy, float uz);
 int psl_set_given_field(psl_grid* grid, const float* host_rho_u);
 /* getSmagorinskyConstant (uniform per grid); 0 disables LES. */
 int psl_set_smagorinsky(psl_grid* grid, float cs);
+/* getSmagorinskyConstant(i, j, k, Info) per cell (include/applyLocalCellUpdate.h:68, e.g.
+ * NACA0012/NACA0012Main.cu:74): host constants x N in cell order (i fastest), each finite
+ * and >= 0 (0: no LES at that cell), evaluated once from the case's hook and kept on the
+ * device (4 bytes per cell, read by every update); NULL returns to the uniform constant.
+ * Used by the plain, customised and scalar-transport updates; the learned closure, when
+ * attached, replaces the Smagorinsky rate altogether.  Not for grids in a batch. */
+int psl_set_smagorinsky_field(psl_grid* grid, const float* host_cs);
 /* The customised update of the reference's rotating-machinery cases
  * (M35Full/applyLocalCellUpdateCustomized.h, M40Impeller/applyLocalCellUpdateCustomized.h)
  * on PS grids.  Selected when a body force is set or the markers hold either of:
@@ -168,6 +175,15 @@ int psl_sphere_force(psl_grid* grid, const psl_sphere_case* sc, double* force3);
  * of getTorque (M35Full/m35Main.cu:176-260, which sums -F_x y + F_y x of forced-velocity
  * cells through its case's forcing hook) for bounce-back bodies; force3 may be NULL. */
 int psl_torque(psl_grid* grid, const int* lo3, const int* hi3, const float* point3, double* torque3, double* force3);
+/* getTorque (M35Full/m35Main.cu:176-260) on a PS grid: over the forced-velocity cells
+ * (marker 0x09) with k >= k_min (the reference's case skips k < 5), the forcing
+ * g = rho (u_given - u) of the cell's stored populations -- the library's forced cells are
+ * driven toward their given velocity, where the reference's case computes its target in
+ * getForcing -- converted to physical force (convertToPhysicalForce: rho_nominal_phys
+ * (res/1000)^4 / dt_phys^2), summed as -g_x y + g_y x with (x, y) = (i res + ox, j res + oy),
+ * divided by 1000 (N mm -> N m).  FP64 sums (the reference sums in FP32).  force3 (may be
+ * NULL): the summed physical forcing. */
+int psl_forcing_torque(psl_grid* grid, int k_min, float rho_nominal_phys, double* torque, double* force3);
 
 /* getFlowReportGeneral (flowReportFunctions.h:2-251) over a grid hierarchy (grids[0]
  * coarsest): section plane `plane` at finest-grid index `cut_index`, cropped to the physical

@@ -41,6 +41,8 @@ class CaseConfig(ctypes.Structure):
         ("noiseAmp", ctypes.c_float),
         ("iSub2_0", ctypes.c_int), ("jSub2_0", ctypes.c_int), ("kSub2_0", ctypes.c_int),
         ("iSub2_1", ctypes.c_int), ("jSub2_1", ctypes.c_int), ("kSub2_1", ctypes.c_int),
+        ("csMode", ctypes.c_int),
+        ("forceR0", ctypes.c_float), ("forceR1", ctypes.c_float), ("forceOmega", ctypes.c_float),
     ]
 
 
@@ -61,6 +63,8 @@ class SphereCase:
     noise: float = 1e-4
     refine: tuple | None = None  # ((i0, j0, k0), (i1, j1, k1)) coarse block, half-open
     refine2: tuple | None = None  # a third level: block on the level-1 grid (its own cells)
+    cs_mode: int = 0  # 0 uniform Smagorinsky constant, 1 outlet sponge (getSmagorinskyConstant per cell)
+    force_annulus: tuple | None = None  # (R0, R1, omega): forced-velocity cells for getTorque (reference build)
 
     def to_ctypes(self) -> CaseConfig:
         c = CaseConfig()
@@ -78,6 +82,9 @@ class SphereCase:
         c.wallMode = self.wall_mode
         c.seed = self.seed
         c.noiseAmp = self.noise
+        c.csMode = self.cs_mode
+        if self.force_annulus:
+            c.forceR0, c.forceR1, c.forceOmega = self.force_annulus
         return c
 
 
@@ -164,6 +171,16 @@ class Sim:
         """fillCoarseGridFromFine on levels `level` and `level` + 1."""
         self.owner._fn("sim_fill_coarse_from_fine")(self.h, int(level))
 
+    def torque(self, level: int = 0) -> float:
+        """The reference's getTorque written for PS grids (reference build only)."""
+        return float(self.owner.lib.ref_sim_torque(self.h, level))
+
+    def export_section(self, level: int, plane: str, cut_index: int, plot_number: int, path: str):
+        """The reference's exportSectionCutPlotGeneral of one level, written to `path`
+        (reference build only)."""
+        planes = {"XY": 0, "ZY": 1, "ZX": 2}
+        self.owner.lib.ref_sim_export_section(self.h, level, planes[plane], cut_index, plot_number, path.encode())
+
 
 class RefLib(_SimLib):
     """The reference's own code (compiled through the TNL shim)."""
@@ -194,11 +211,28 @@ class RefLib(_SimLib):
         L.ref_sim_get_T.argtypes = [vp, vp]
         L.ref_rescale.argtypes = [vp, i]
         L.ref_streaming.argtypes = [i, i, i, vp]
+        L.ref_smagorinsky_constants.argtypes = [ctypes.POINTER(CaseConfig), i, i, i, i, vp]
+        L.ref_sim_export_section.argtypes = [vp, i, i, i, i, ctypes.c_char_p]
+        L.ref_sim_torque.argtypes = [vp, i]
+        L.ref_sim_torque.restype = f
+        L.ref_export_history.argtypes = [vp, i, i, ctypes.c_char_p]
         for n in ("ref_sim_periodic_x", "ref_sim_periodic_y", "ref_sim_streaming"):
             getattr(L, n).argtypes = [vp, i]
 
     def _create(self, cfg, **kw):
         return self.lib.ref_sim_create(ctypes.byref(cfg))
+
+    def export_history(self, values, current_iteration: int, path: str):
+        """exportHistoryData of the reference, written to `path`."""
+        v = np.ascontiguousarray(values, dtype=np.float32)
+        self.lib.ref_export_history(v.ctypes.data, v.size, current_iteration, path.encode())
+
+    def smagorinsky_constants(self, case: SphereCase, grid_id: int, nx: int, ny: int, nz: int) -> np.ndarray:
+        """The case's getSmagorinskyConstant hook over every cell of a grid (cell order)."""
+        out = np.zeros(nx * ny * nz, dtype=np.float32)
+        cfg = case.to_ctypes()
+        self.lib.ref_smagorinsky_constants(ctypes.byref(cfg), grid_id, nx, ny, nz, out.ctypes.data)
+        return out
 
     def sim(self, case: SphereCase) -> Sim:
         return Sim(self, case)

@@ -409,7 +409,7 @@ template <typename T>
 static void localUpdate(Sim<T>& sim, Grid<T>& g) {
   const Info& I = g.info;
   const CaseConfig& c = sim.cfg;
-  const T nu = T(I.nu), cs = T(c.smagorinsky);
+  const T nu = T(I.nu);
   const T rhoGiven = T(1), uxGiven = T(c.uIn), uyGiven = T(0), uzGiven = T(0);
 #pragma omp parallel for schedule(static)
   for (long long cell = 0; cell < I.n; ++cell) {
@@ -437,7 +437,7 @@ static void localUpdate(Sim<T>& sim, Grid<T>& g) {
           mbbc(n, f, rho, ux, uy, uz);
         }
       }
-      collide(f, nu, cs);
+      collide(f, nu, T(smagorinskyConstant(c, I.level, I.nx, i)));
     }
     for (int q = 0; q < 27; ++q) g.f[(size_t)q * I.n + a[q]] = f[q];
   }

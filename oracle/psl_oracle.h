@@ -43,6 +43,18 @@ struct CaseConfig {
   float noiseAmp;
   int iSub2_0, jSub2_0, kSub2_0;  // third level: refinement block on the level-1 grid
   int iSub2_1, jSub2_1, kSub2_1;
+  int csMode;  // 0 uniform Smagorinsky constant, 1 outlet sponge on the coarse grid
+  float forceR0, forceR1, forceOmega;  // forced-velocity annulus (read by the reference build's getTorque only)
 };
+
+// getSmagorinskyConstant of the sphere cases (oracle/ref_cases.cpp): csMode 1 raises C_s
+// linearly from i = 3 Nx / 4 to four times its value at the outlet plane (coarse grid).
+inline float smagorinskyConstant(const CaseConfig& c, int gridID, int nx, int i) {
+  if (c.csMode == 1 && gridID == 0) {
+    const int i0 = (3 * nx) / 4;
+    if (i > i0) return c.smagorinsky * (1.f + 3.f * (float)(i - i0) / (float)(nx - 1 - i0));
+  }
+  return c.smagorinsky;
+}
 
 }  // namespace oracle

@@ -4,7 +4,8 @@
 // project's own headers UNMODIFIED (include/types.h, include/cellFunctions.h,
 // include/applyStreaming.h, include/applyCollision.h, include/boundaryConditions/*.h,
 // include/applyLocalCellUpdate.h, include/fillEquilibrium.h,
-// include/gridRefinementFunctions.h, and the free-slip generator output
+// include/gridRefinementFunctions.h, include/scalarTransportFunctions.h,
+// include/plotter/exportSectionCutPlot.h, and the free-slip generator output
 // symbolicHelperTools/CppCodeGenerator/results/applyMirror.h that the reference's drivers
 // include but its include/ folder lacks).  It supplies what a reference case file
 // supplies: physical constants, the per-case hook functions (getMarkers,
@@ -64,6 +65,9 @@ extern "C" struct RefCaseConfig {
   float noiseAmp;
   int iSub2_0, jSub2_0, kSub2_0;  // third level: refinement block on the level-1 grid
   int iSub2_1, jSub2_1, kSub2_1;
+  int csMode;              // 0 uniform Smagorinsky constant, 1 outlet sponge (see getSmagorinskyConstant)
+  float forceR0, forceR1;  // forced-velocity annulus around the sphere's z axis (coarse grid; R1 = 0: none)
+  float forceOmega;        // its target: solid rotation at this angular velocity (lattice units)
 };
 
 static RefCaseConfig g_case;
@@ -104,6 +108,10 @@ __cuda_callable__ void getMarkers(const int& iCell, const int& jCell, const int&
     else if (isFreeSlipWall(iCell, jCell, kCell, Info)) { /* mirror: no given moments */ }
     else Marker.fluid = 1;
   }
+  if (g_case.forceR1 > 0.f && Marker.fluid) {  // the annulus read by getTorque (the PS update ignores the flag)
+    const float a2 = (xPhys - g_case.sphereX) * (xPhys - g_case.sphereX) + (yPhys - g_case.sphereY) * (yPhys - g_case.sphereY);
+    if (a2 >= g_case.forceR0 * g_case.forceR0 && a2 <= g_case.forceR1 * g_case.forceR1) Marker.forcedVelocity = 1;
+  }
 }
 
 __cuda_callable__ void getGivenRhoUxUyUz(const int& iCell, const int& jCell, const int& kCell, float& rho, float& ux,
@@ -114,8 +122,15 @@ __cuda_callable__ void getGivenRhoUxUyUz(const int& iCell, const int& jCell, con
   uz = 0.f;
 }
 
+// csMode 1, a sponge layer ahead of the outlet on the coarse grid: C_s rises linearly from
+// its value at i = 3 Nx / 4 to four times that at the outlet plane.  Every operation is one
+// FP32 rounding, so a field built from the same expression holds the same numbers.
 __cuda_callable__ float getSmagorinskyConstant(const int& iCell, const int& jCell, const int& kCell,
                                                const InfoStruct& Info) {
+  if (g_case.csMode == 1 && Info.gridID == 0) {
+    const int i0 = (3 * Info.cellCountX) / 4;
+    if (iCell > i0) return g_case.smagorinsky * (1.f + 3.f * (float)(iCell - i0) / (float)(Info.cellCountX - 1 - i0));
+  }
   return g_case.smagorinsky;
 }
 
@@ -165,6 +180,73 @@ __host__ __device__ void applyScalarTransportGivenT(float (&T)[27], float& given
 #include "include/fillEquilibrium.h"
 #include "include/gridRefinementFunctions.h"
 #include "include/boundaryConditions/periodicXY.h"
+
+// The plotter exports (include/plotter/exportSectionCutPlot.h) open fixed /dev/shm paths
+// with fopen; for this build fopen is routed through a function that substitutes a path
+// the caller chooses, so the header's own code writes the file a test then compares.
+#include <cstdio>
+#include <iostream>
+static const char* g_export_path = nullptr;
+static FILE* ref_export_fopen(const char* path, const char* mode) {
+  return std::fopen(g_export_path ? g_export_path : path, mode);
+}
+// The header's DIAD down-sampling calls an unqualified integer max, which nvcc's headers
+// provide in the global namespace; the host build takes std::max.
+using std::max;
+#define fopen ref_export_fopen
+#include "include/plotter/exportSectionCutPlot.h"
+#undef fopen
+
+// getForcing (the hook of M35Full/m35Main.cu:101-119) of the forced-velocity annulus:
+// rho (u_target - u) toward solid rotation about the sphere's z axis.
+__cuda_callable__ void getForcing(const int& iCell, const int& jCell, const int& kCell, const float (&f)[27], float& gx,
+                                  float& gy, float& gz, const InfoStruct& Info) {
+  float rho, ux, uy, uz;
+  getRhoUxUyUz(rho, ux, uy, uz, f);
+  float x, y, z;
+  getXYZFromIJKCellIndex(iCell, jCell, kCell, x, y, z, Info);
+  const float uxTarget = -g_case.forceOmega * (y - g_case.sphereY);
+  const float uyTarget = g_case.forceOmega * (x - g_case.sphereX);
+  const float uzTarget = 0.f;
+  gx = rho * (uxTarget - ux);
+  gy = rho * (uyTarget - uy);
+  gz = rho * (uzTarget - uz);
+}
+
+// getTorque (M35Full/m35Main.cu:176-260) written for a PS grid: the same fetch and FP32
+// reduction over the forced-velocity cells above the first five layers, the cell's
+// populations read through getShiftedIndex instead of the Esotwist neighbour arrays.
+float getTorque(GridStruct& Grid) {
+  auto fArrayView = Grid.fArray.getConstView();
+  auto shifterView = Grid.shifter.getConstView();
+  InfoStruct Info = Grid.Info;
+  auto fetch = [=] __cuda_callable__(const int cell) {
+    int iCell, jCell, kCell;
+    getIJKCellIndex(cell, iCell, jCell, kCell, Info);
+    if (kCell < 5) return 0.f;
+    MarkerStruct Marker;
+    getMarkers(iCell, jCell, kCell, Marker, Info);
+    if (Marker.movingBounceback) return 0.f;
+    if (!Marker.forcedVelocity) return 0.f;
+    float x, y, z;
+    getXYZFromIJKCellIndex(iCell, jCell, kCell, x, y, z, Info);
+    int shiftedIndex[27];
+    getShiftedIndex(cell, shiftedIndex, shifterView, Info);
+    float f[27];
+    for (int direction = 0; direction < 27; direction++) f[direction] = fArrayView(direction, shiftedIndex[direction]);
+    float gx = 0.f;
+    float gy = 0.f;
+    float gz = 0.f;
+    getForcing(iCell, jCell, kCell, f, gx, gy, gz, Info);
+    convertToPhysicalForce(gx, gy, gz, Info);
+    float T = -gx * y + gy * x;
+    return T;
+  };
+  auto reduction = [] __cuda_callable__(const float& a, const float& b) { return a + b; };
+  float TSum = TNL::Algorithms::reduce<TNL::Devices::Cuda>(0, Info.cellCount, fetch, reduction, 0.f);
+  TSum = TSum / 1000.f;  // converting from Nmm to Nm
+  return TSum;
+}
 
 // Customized PS update for free-slip walls, in the reference's per-case customisation
 // style (M35Full/m35Main.cu:134-135 swaps in a case's own update): identical to
@@ -283,6 +365,42 @@ static void updateLevel(RefSim& sim, int level) {
 }
 
 extern "C" {
+
+// exportSectionCutPlotGeneral (exportSectionCutPlot.h:2-89) of one level, written to `path`.
+void ref_sim_export_section(void* p, int level, int plane, int cutIndex, int plotNumber, const char* path) {
+  RefSim* sim = static_cast<RefSim*>(p);
+  g_export_path = path;
+  exportSectionCutPlotGeneral(sim->grids[level], cutIndex, plotNumber, static_cast<PlaneEnum>(plane));
+  g_export_path = nullptr;
+}
+
+// getTorque of one level (forced-velocity annulus of the case).
+float ref_sim_torque(void* p, int level) {
+  RefSim* sim = static_cast<RefSim*>(p);
+  return getTorque(sim->grids[level]);
+}
+
+// exportHistoryData (exportSectionCutPlot.h:994-1001), written to `path`.
+void ref_export_history(const float* values, int count, int currentIteration, const char* path) {
+  std::vector<float> history(values, values + count);
+  g_export_path = path;
+  exportHistoryData(history, currentIteration);
+  g_export_path = nullptr;
+}
+
+// getSmagorinskyConstant(i, j, k, Info) of every cell of a grid, cell order (i fastest).
+void ref_smagorinsky_constants(const RefCaseConfig* cfg, int gridID, int nx, int ny, int nz, float* out) {
+  g_case = *cfg;
+  InfoStruct Info;
+  Info.gridID = gridID;
+  Info.cellCountX = nx;
+  Info.cellCountY = ny;
+  Info.cellCountZ = nz;
+  Info.cellCount = nx * ny * nz;
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) out[((size_t)k * ny + j) * nx + i] = getSmagorinskyConstant(i, j, k, Info);
+}
 
 void* ref_sim_create(const RefCaseConfig* cfg) {
   g_case = *cfg;

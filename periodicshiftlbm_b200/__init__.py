@@ -22,6 +22,7 @@ from .grid import (  # noqa: F401
     fillEquilibriumFromFunction,
     getSphereDrag,
     getFlowReport,
+    getForcingTorque,
     getSphereForce,
     getTorque,
     setBodyForce,

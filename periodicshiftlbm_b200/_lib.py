@@ -91,6 +91,9 @@ _SIGNATURES = {
     "psl_set_given": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float]),
     "psl_set_given_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_set_smagorinsky": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_float]),
+    "psl_set_smagorinsky_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "psl_forcing_torque": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_void_p,
+                                          ctypes.c_void_p]),
     "psl_fill_equilibrium_sphere": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PslSphereCase)]),
     "psl_fill_equilibrium_uniform": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                                     ctypes.c_float]),

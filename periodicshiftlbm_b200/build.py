@@ -46,10 +46,29 @@ def _stale(target: str, deps) -> bool:
 
 
 def build_library(force: bool = False, verbose: bool = False) -> str:
+    """Compile each translation unit to an object in parallel (one nvcc per file), then
+    link the shared library."""
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(REPO, "include", "psl.h")]
     if not force and not _stale(LIB, deps):
         return LIB
-    cmd = [_nvcc(), *NVCC_FLAGS, "-I", os.path.join(REPO, "include"), "-I", CSRC, *SOURCES, "-o", LIB + ".tmp"]
+    from concurrent.futures import ThreadPoolExecutor
+
+    objdir = os.path.join(PKG, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    incs = ["-I", os.path.join(REPO, "include"), "-I", CSRC]
+
+    def compile_one(src: str) -> str:
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        cmd = [_nvcc(), *compile_flags, *incs, "-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as pool:
+        objs = list(pool.map(compile_one, SOURCES))
+    cmd = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs, "-o", LIB + ".tmp"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
@@ -57,10 +76,23 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+def reference_checkout() -> str | None:
+    """The reference checkout the CPU checker is compiled from: PSL_REFERENCE_DIR, else the
+    location the build machine keeps it at; None where neither exists (a GPU box uses the
+    prebuilt oracle/_ref)."""
+    for cand in (os.environ.get("PSL_REFERENCE_DIR"), "/root/reference"):
+        if cand and os.path.isdir(os.path.join(cand, "include")):
+            return cand
+    return None
+
+
 def build_oracle(verbose: bool = False) -> None:
     """The CPU checkers (test infrastructure): liboracle.so and, if the reference
     checkout exists on this machine, oracle/_ref/libpsl_ref.so."""
     cmd = ["make", "-s", "-C", os.path.join(REPO, "oracle"), "all"]
+    ref = reference_checkout()
+    if ref:
+        cmd.append(f"REF={ref}")
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -14,7 +14,9 @@ from __future__ import annotations
 
 from dataclasses import dataclass, replace
 
-from .grid import GridStruct, InfoStruct, SphereCase, fillEquilibriumFromFunction, setSphereCase
+import numpy as np
+
+from .grid import GridStruct, InfoStruct, SphereCase, fillEquilibriumFromFunction, setSmagorinskyConstant, setSphereCase
 
 
 @dataclass(frozen=True)
@@ -33,6 +35,7 @@ class SphereConfig:
     noise: float = 1e-4
     refine: tuple | None = None  # ((i0, j0, k0), (i1, j1, k1)) coarse block, half-open
     refine2: tuple | None = None  # a third level: block on the level-1 grid (its own cells)
+    cs_mode: int = 0  # 0 uniform C_s; 1 outlet sponge on the coarse grid (sponge_smagorinsky)
 
     def case(self) -> SphereCase:
         return SphereCase(sphere=tuple(float(v) for v in self.sphere), radius=float(self.radius), u_in=self.u_in,
@@ -98,14 +101,31 @@ def config2(scale: float = 1.0, **kw) -> SphereConfig:
     return replace(c, **kw)
 
 
+def sponge_smagorinsky(info: InfoStruct, cs: float) -> np.ndarray:
+    """getSmagorinskyConstant(i, j, k, Info) of a sponge layer ahead of the outlet, for every
+    cell of a grid in cell order: C_s rises linearly from `cs` at i = 3 Nx / 4 to 4 cs at
+    the outlet plane.  Evaluated in FP32 with one rounding per operation, in the order of
+    the C++ hook cs * (1 + 3 (i - i0) / (Nx - 1 - i0)), so both give the same numbers."""
+    nx, ny, nz = info.cellCountX, info.cellCountY, info.cellCountZ
+    i0 = (3 * nx) // 4
+    i = np.arange(nx)
+    ramp = np.float32(3.0) * (i - i0).astype(np.float32)
+    ramp = ramp / np.float32(nx - 1 - i0)
+    row = np.where(i > i0, np.float32(cs) * (np.float32(1.0) + ramp), np.float32(cs)).astype(np.float32)
+    return np.broadcast_to(row, (nz, ny, nx)).reshape(-1).copy()
+
+
 def make_sphere_grids(cfg: SphereConfig, storage: str = "f32") -> tuple:
-    """Allocate the grids of `cfg`, evaluate the case hooks into markers and fill the
-    start state.  Returns (grids, case)."""
+    """Allocate the grids of `cfg`, evaluate the case hooks into markers (and, for
+    cs_mode 1, the coarse grid's per-cell Smagorinsky constants) and fill the start state.
+    Returns (grids, case)."""
     case = cfg.case()
     grids = []
     for info in cfg.infos():
         g = GridStruct(info, storage=storage)
         setSphereCase(g, case)
+        if cfg.cs_mode == 1 and info.gridID == 0:
+            setSmagorinskyConstant(g, sponge_smagorinsky(info, cfg.smagorinsky))
         fillEquilibriumFromFunction(g, case)
         grids.append(g)
     return grids, case

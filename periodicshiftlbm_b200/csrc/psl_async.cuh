@@ -55,6 +55,12 @@ __device__ __forceinline__ void bulk_store(void* gmem_dst, const void* smem_src,
                : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Wait until at most N of this thread's most recent bulk groups are still reading their
+// shared-memory source (the older ones may still be writing to global memory).
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
 // Wait until every committed bulk group of this thread has completed (writes done).
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 

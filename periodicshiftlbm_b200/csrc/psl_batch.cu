@@ -237,6 +237,8 @@ int psl_batch_create(psl_grid* const* grids, int count, psl_batch** out) {
     BATCH_CHECK(g->info.i_subgrid_end <= g->info.i_subgrid_start, PSL_ERR_INVALID,
                 "psl_batch_create: grids with a refinement block are not batched");
     BATCH_CHECK(27ull * g->stride + g->n < (1ull << 32), PSL_ERR_INVALID, "psl_batch_create: grid too large");
+    BATCH_CHECK(!g->cs_field, PSL_ERR_INVALID,
+                "psl_batch_create: grids with a per-cell Smagorinsky field are not batched");
   }
   DeviceGuard dg(grids[0]->device);
   psl_batch* b = new psl_batch();

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -13,7 +14,7 @@
 #include "psl.h"
 #include "psl_internal.h"
 #include "psl_kernels.cuh"
-#include "psl_step_tiled.cuh"
+#include "psl_step_pipe.cuh"
 
 using namespace psl;
 
@@ -149,10 +150,6 @@ int psl_grid_create(const psl_info* info, int storage, psl_grid** out) {
   g->n = (uint32_t)n;
   g->storage = storage;
   g->stride = ((size_t)n + 63) / 64 * 64;
-  // PSL_STEP_KERNEL=tiled selects the bulk-copy tiled update kernel where it applies
-  // (N % 128 == 0); the default is the one-thread-per-cell kernel.
-  const char* kernel_choice = getenv("PSL_STEP_KERNEL");
-  g->tiled = kernel_choice && std::string(kernel_choice) == "tiled";
   cudaGetDevice(&g->device);
   const size_t bytes = 27 * g->stride * storage_bytes(storage);
   cudaError_t e = cudaMalloc(&g->f, bytes);
@@ -184,6 +181,7 @@ int psl_grid_destroy(psl_grid* g) {
   if (g->mlp) cudaFree(g->mlp);
   if (g->T) cudaFree(g->T);
   if (g->givenT) cudaFree(g->givenT);
+  if (g->cs_field) cudaFree(g->cs_field);
   delete g;
   return PSL_OK;
 }
@@ -382,6 +380,34 @@ int psl_set_smagorinsky(psl_grid* g, float cs) {
   return PSL_OK;
 }
 
+int psl_set_smagorinsky_field(psl_grid* g, const float* host_cs) {
+  PSL_CHECK(g, PSL_ERR_INVALID, "psl_set_smagorinsky_field: null grid");
+  DeviceGuard dg(g->device);
+  if (!host_cs) {
+    if (g->cs_field) {
+      PSL_CUDA(cudaStreamSynchronize(g->stream));
+      cudaFree(g->cs_field);
+      g->cs_field = nullptr;
+    }
+    return PSL_OK;
+  }
+  for (uint32_t c = 0; c < g->n; ++c)
+    PSL_CHECK(std::isfinite(host_cs[c]) && host_cs[c] >= 0.f, PSL_ERR_INVALID,
+              "psl_set_smagorinsky_field: every constant must be finite and >= 0");
+  if (!g->cs_field) {
+    cudaError_t e = cudaMalloc(&g->cs_field, g->stride * sizeof(float));
+    if (e != cudaSuccess) {
+      g->cs_field = nullptr;
+      cudaGetLastError();
+      return fail(PSL_ERR_NOMEM, std::string("psl_set_smagorinsky_field: ") + cudaGetErrorString(e));
+    }
+    PSL_CUDA(cudaMemsetAsync(g->cs_field, 0, g->stride * sizeof(float), g->stream));
+  }
+  PSL_CUDA(cudaMemcpyAsync(g->cs_field, host_cs, (size_t)g->n * sizeof(float), cudaMemcpyHostToDevice, g->stream));
+  PSL_CUDA(cudaStreamSynchronize(g->stream));
+  return PSL_OK;
+}
+
 // ---- per-step update ----
 template <typename Case>
 static int fill_eq(psl_grid* g, const Case& c) {
@@ -454,13 +480,76 @@ static RelaxationT<T> relaxation(const psl_grid* g) {
   return rx;
 }
 
+// Resident CTAs of the pipelined update per SM, per device and kernel form.  The first
+// call on a device also raises the kernel's dynamic shared-memory limit to what it uses
+// (static + dynamic above 48 KB needs the opt-in); later launches read the cache.
+static int pipe_blocks_per_sm(const void* kernel, size_t smem, int device, int form) {
+  static std::atomic<int> cache[64][8];
+  std::atomic<int>& slot = cache[device & 63][form & 7];
+  int v = slot.load(std::memory_order_relaxed);
+  if (v > 0) return v;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, kPipeCells, smem) != cudaSuccess) return 0;
+  slot.store(v, std::memory_order_relaxed);
+  return v;
+}
+
+// The pipelined update (psl_step_pipe.cuh) where it applies: FP32 / FP16 / BF16 storage and
+// N a multiple of 16 bytes of elements.  Returns false when the grid takes the
+// one-thread-per-cell kernel instead.
 template <typename S>
-static void launch_step(psl_grid* g) {
+static bool launch_pipe(psl_grid* g, cudaError_t* err) {
+  if constexpr (S::kind == kStoreF64) {
+    return false;
+  } else {
+    using Lay = PipeLayout<S>;
+    if (g->n % Lay::V) return false;
+    PipeParams<S> p;
+    p.base = static_cast<typename S::type*>(g->f);
+    p.stride = (uint32_t)g->stride;
+    p.n = g->n;
+    p.ntiles = (g->n + kPipeCells - 1) / kPipeCells;
+    p.stage_bytes = g->cs_field ? Lay::kStageBytesCs : Lay::kStageBytes;
+    p.extra_bytes = 0;
+    for (int q = 0; q < 27; ++q) {
+      const uint32_t rem = g->shift[q] % Lay::V;
+      p.shift[q] = g->shift[q];
+      p.soff[q] = (uint32_t)(q * Lay::kRowBytes) + rem * Lay::E;
+      if (rem) p.extra_bytes += 16;
+    }
+    p.marker = g->marker;
+    p.given = g->given;
+    p.given_uniform = g->given_uniform;
+    p.cs = g->cs_field;
+    p.rx = relaxation<float>(g);
+    p.health = g->health;
+    const size_t smem = (size_t)Lay::kStages * (p.stage_bytes + 8);
+    const int per_sm = pipe_blocks_per_sm((const void*)step_pipe_kernel<S>, smem, g->device,
+                                          2 * S::kind + (g->cs_field ? 1 : 0));
+    int sms = 0;
+    *err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+    if (*err != cudaSuccess) return true;
+    if (per_sm <= 0) {
+      *err = cudaErrorInvalidConfiguration;
+      return true;
+    }
+    const unsigned int blocks = std::min<unsigned int>(p.ntiles, (unsigned int)(per_sm * sms));
+    step_pipe_kernel<S><<<blocks, kPipeCells, smem, g->stream>>>(p);
+    *err = cudaGetLastError();
+    return true;
+  }
+}
+
+template <typename S>
+static cudaError_t launch_step(psl_grid* g) {
+  cudaError_t err = cudaSuccess;
+  if (launch_pipe<S>(g, &err)) return err;
   StepParams<S> p;
   p.g = view<S>(g);
   p.marker = g->marker;
   p.given = g->given;
   p.given_uniform = g->given_uniform;
+  p.cs = g->cs_field;
   p.rx = relaxation<typename S::calc>(g);
   p.health = g->health;
   p.ri.base = static_cast<typename S::type*>(g->f);
@@ -470,16 +559,11 @@ static void launch_step(psl_grid* g) {
     p.ri.lim[q] = g->n - g->shift[q];
   }
   const bool row_index = 27 * g->stride + g->n < (1ull << 32);
-  if constexpr (S::kind != kStoreF64) {
-    if (g->tiled && g->n % kTile == 0) {
-      step_tiled_kernel<S><<<g->n / kTile, kTile, 0, g->stream>>>(p);
-      return;
-    }
-  }
   if (row_index)
     step_kernel<S, true><<<blocks_for(g->n, kStepThreads), kStepThreads, 0, g->stream>>>(p);
   else
     step_kernel<S, false><<<blocks_for(g->n, kStepThreads), kStepThreads, 0, g->stream>>>(p);
+  return cudaGetLastError();
 }
 
 int psl_apply_local_cell_update(psl_grid* g) {
@@ -501,6 +585,7 @@ int psl_apply_local_cell_update(psl_grid* g) {
         sp.base.marker = g->marker;
         sp.base.given = g->given;
         sp.base.given_uniform = g->given_uniform;
+        sp.base.cs = g->cs_field;
         sp.base.rx = relaxation<float>(g);
         sp.base.health = g->health;
         sp.T.base = g->T;
@@ -535,6 +620,7 @@ int psl_apply_local_cell_update(psl_grid* g) {
         cp.base.marker = g->marker;
         cp.base.given = g->given;
         cp.base.given_uniform = g->given_uniform;
+        cp.base.cs = g->cs_field;
         cp.base.rx = relaxation<float>(g);
         cp.base.health = g->health;
         cp.body = g->body;
@@ -545,11 +631,7 @@ int psl_apply_local_cell_update(psl_grid* g) {
     PSL_CUDA(cudaGetLastError());
     return PSL_OK;
   }
-  with_storage(g->storage, [&](auto s) {
-    launch_step<decltype(s)>(g);
-    return 0;
-  });
-  PSL_CUDA(cudaGetLastError());
+  PSL_CUDA(with_storage(g->storage, [&](auto s) { return launch_step<decltype(s)>(g); }));
   return PSL_OK;
 }
 

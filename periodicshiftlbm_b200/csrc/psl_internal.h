@@ -39,12 +39,12 @@ struct psl_grid {
   float4* given = nullptr;
   float4 given_uniform = make_float4(1.f, 0.f, 0.f, 0.f);
   float cs = 0.f;
+  float* cs_field = nullptr;        // per-cell Smagorinsky constants (getSmagorinskyConstant), or null
   uint32_t shift[27] = {};
   cudaStream_t stream = 0;
   unsigned int* health = nullptr;   // [0] health bits, [1] barrier counter
   double* scratch = nullptr;        // force partials (kForceBlocks x 3) + result (3)
   int device = 0;
-  bool tiled = false;               // bulk-copy tiled update kernel (N % 128 == 0)
   int batched = 0;                  // member of this many live batches (psl_batch.cu)
   float3 body = make_float3(0.f, 0.f, 0.f);  // uniform body force (customised update)
   bool custom_markers = false;      // moving-wall or forced-velocity markers present

@@ -56,9 +56,19 @@ struct StepParams {
   const uint8_t* marker;
   const float4* given;   // per-cell (rho, ux, uy, uz) for boundary cells, or null
   float4 given_uniform;  // used when `given` is null
+  const float* cs;       // per-cell Smagorinsky constant (getSmagorinskyConstant), or null: rx.cs18
   RelaxationT<typename S::calc> rx;
   unsigned int* health;  // bit 0 set when a collided cell's density is not finite/positive
 };
+
+// The relaxation parameters of one cell: the grid's, with the cell's own Smagorinsky
+// constant when the grid has a per-cell field.
+template <typename T>
+__device__ __forceinline__ RelaxationT<T> cell_relaxation(const RelaxationT<T>& rx, const float* cs, uint32_t cell) {
+  RelaxationT<T> r = rx;
+  if (cs) r.cs18 = T(18) * T(cs[cell]);
+  return r;
+}
 
 // The boundary branch runs for ~2% of cells; keeping it out of line keeps the hot path's
 // instruction footprint small.  (applyLocalCellUpdate.h:41-67)
@@ -77,21 +87,25 @@ static __device__ __noinline__ void apply_boundary_out_of_line(uint8_t m, T* pop
   bc::mbbc(normal, f, rho, ux, uy, uz);
 }
 
-// The call site: the populations go through the thread's own slot in shared memory
-// (kSlots >= the block's threads), written and read inside the boundary branch only.
-// Passing the caller's array by reference would take its address, and nvcc then keeps it in
-// local memory for every cell (a stack write of all 27 populations per fluid cell too); a
-// copy in local memory inside the branch still cost a warp holding one inflow cell 8% of the
-// update launch on a 512-wide grid, the shared-memory slot 3%.
-template <int kSlots = kStepThreads, typename T>
-__device__ __forceinline__ void apply_boundary(uint8_t m, T (&f)[27], float4 given) {
-  __shared__ T slot[kSlots][27];
-  T* mine = slot[threadIdx.x];
+// The call site: the populations go through the thread's own slot in shared memory,
+// written and read inside the boundary branch only.  Passing the caller's array by
+// reference would take its address, and nvcc then keeps it in local memory for every cell
+// (a stack write of all 27 populations per fluid cell too); a copy in local memory inside
+// the branch still cost a warp holding one inflow cell 8% of the update launch on a
+// 512-wide grid, the shared-memory slot 3%.
+template <typename T>
+__device__ __forceinline__ void apply_boundary_at(uint8_t m, T (&f)[27], float4 given, T* mine) {
 #pragma unroll
   for (int q = 0; q < 27; ++q) mine[q] = f[q];
   apply_boundary_out_of_line(m, mine, given);
 #pragma unroll
   for (int q = 0; q < 27; ++q) f[q] = mine[q];
+}
+// ... with a kernel-wide slot array of kSlots >= the block's threads.
+template <int kSlots = kStepThreads, typename T>
+__device__ __forceinline__ void apply_boundary(uint8_t m, T (&f)[27], float4 given) {
+  __shared__ T slot[kSlots][27];
+  apply_boundary_at(m, f, given, slot[threadIdx.x]);
 }
 
 template <typename S, int Q = 0>
@@ -172,7 +186,7 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constan
     }
   } else {
     if (kind != kFluid) apply_boundary(m, f, p.given ? p.given[cell] : p.given_uniform);
-    collide<false>(f, p.rx);
+    collide<false>(f, cell_relaxation(p.rx, p.cs, cell));
     if (p.health) {
       const T r = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6];
       if (!(r > T(0) && r < T(1.0e30))) atomicOr(p.health, 1u);
@@ -257,7 +271,7 @@ __global__ void __launch_bounds__(kStepThreads) step_custom_kernel(const __grid_
       gy += rho * (gv.z - jy / rho);
       gz += rho * (gv.w - jz / rho);
     }
-    collide<true>(f, p.rx, gx, gy, gz);
+    collide<true>(f, cell_relaxation(p.rx, p.cs, cell), gx, gy, gz);
     if (p.health) {
       const float r = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6];
       if (!(r > 0.f && r < 1.0e30f)) atomicOr(p.health, 1u);
@@ -342,7 +356,7 @@ __global__ void __launch_bounds__(kStepThreads) step_scalar_kernel(const __grid_
         for (int q = 0; q < 27; ++q) T[q] = tg;
       }
     }
-    collide<false>(f, p.rx);
+    collide<false>(f, cell_relaxation(p.rx, p.cs, cell));
     scalar_collision(f, T, sp.tauT);
     if (p.health) {
       const float r = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6];

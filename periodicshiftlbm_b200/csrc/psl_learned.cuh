@@ -1,27 +1,27 @@
 // The update kernels with the learned subgrid closure fused into the collision.
 //
-// Same per-cell work as step_kernel (applyLocalCellUpdate.h:1-74) except the relaxation
-// rate: the cumulant collision's second-order central moments feed the per-cell MLP,
-// whose eddy viscosity sets
+// Same per-cell work as the plain update (applyLocalCellUpdate.h:1-74) except the
+// relaxation rate: the cell's second-order central moments feed the per-cell MLP, whose
+// eddy viscosity sets
 //     omega = 1 / (3 (nu + nu_t) + 1/2)
-// in place of the Smagorinsky rate of include/cellFunctions.h:157-198.  In the tcgen05
-// kernel, a cell whose closure evaluation timed out (bounded wait) keeps the Smagorinsky
-// rate.
+// in place of the Smagorinsky rate of include/cellFunctions.h:157-198.
 //
-// Two evaluations of the closure, one kernel each (same arithmetic around them):
-//   step_learned_warp_kernel  per-warp tensor-core MMAs (psl_mlp_warp.cuh), the default;
-//   step_learned_kernel       CTA-wide tcgen05 MMAs with TMEM accumulators (psl_mlp.cuh).
-// Both run one 128-cell tile per CTA (the tcgen05 kernel stages its weights in shared memory
-// and allocates and frees its 32 TMEM columns per CTA; the per-warp kernel reads its weights
-// from global memory in fragment order, without a CTA barrier): a persistent loop
-// over tiles made the compiler keep the 54 row offsets of the RowIndex in registers across
-// iterations (120 registers against 72 for one tile per CTA).  Every thread takes part in
-// its tile's MMAs (skip, solid and out-of-range cells with zero features), so the warp- or
-// CTA-wide steps inside the closure are reached by all.
+// The closure is evaluated per warp with tensor-core MMAs (psl_mlp_warp.cuh) inside two
+// kernels:
+//   step_pipe_learned_kernel  the pipelined tile update (psl_step_pipe.cuh): the cell's
+//                             moments come from its stored populations in shared memory,
+//                             the collision runs on g = f - w (psl_collision_g.cuh);
+//   step_learned_warp_kernel  one thread per cell with its own loads, for grids the
+//                             pipeline does not take (N not a multiple of 16 bytes of
+//                             elements).
+// Every thread takes part in its warp's MMAs (skip, solid and out-of-range cells with zero
+// features), so the warp-wide steps inside the closure are reached by all lanes.  The
+// CTA-wide tcgen05 evaluation (psl_mlp.cuh) serves the closure's batched inference.
 #pragma once
 #include "psl_kernels.cuh"
 #include "psl_mlp.cuh"
 #include "psl_mlp_warp.cuh"
+#include "psl_step_pipe.cuh"
 
 namespace psl {
 
@@ -31,10 +31,8 @@ struct LearnedParams {
   const uint8_t* marker;
   const float4* given;
   float4 given_uniform;
-  RelaxationT<float> rx;    // Smagorinsky fallback
-  const MlpDevice* mlp;      // tcgen05 layout
-  const MlpFrag* mlpw;       // per-warp layout (fragment order, global memory)
-  MlpScalars sc;             // normalisation, b3, output scale of the per-warp path
+  const MlpFrag* mlpw;       // fragment order, global memory
+  MlpScalars sc;             // normalisation, b3, output scale
   float nu;                 // lattice viscosity of the grid
   float width;              // filter width fed to the closure (cell size / coarsest cell size)
   uint32_t n;
@@ -42,46 +40,93 @@ struct LearnedParams {
 };
 
 template <typename S>
-__global__ void __launch_bounds__(kMlpRows) step_learned_kernel(const __grid_constant__ LearnedParams<S> p) {
-  __shared__ MlpShared s;
-  mlp_cta_setup(s, p.mlp);
-  uint32_t phase = 0;
-  {
-    const uint32_t cell = blockIdx.x * kMlpRows + threadIdx.x;
-    const uint8_t m = cell < p.n ? p.marker[cell] : make_marker(kSkip, 0);
+struct PipeLearnedParams {
+  PipeParams<S> base;
+  const MlpFrag* mlpw;
+  MlpScalars sc;
+  float nu;
+  float width;
+};
+
+// The closure's features from D = C - rho/3 I (the g-form moments): the same quantities
+// as mlp_features (Pi_neq = D / rho, its trace, norm and det / |Pi|^2, the filter width).
+__device__ __forceinline__ void mlp_features_d(const CellMomentsG& m, float width, float (&x)[kMlpIn]) {
+  const float r = m.inv_rho;
+  const float pxx = m.dxx * r, pyy = m.dyy * r, pzz = m.dzz * r;
+  const float pxy = m.dxy * r, pxz = m.dxz * r, pyz = m.dyz * r;
+  const float n2 = pxx * pxx + pyy * pyy + pzz * pzz + 2.f * (pxy * pxy + pxz * pxz + pyz * pyz);
+  const float det = pxx * (pyy * pzz - pyz * pyz) - pxy * (pxy * pzz - pyz * pxz) + pxz * (pxy * pyz - pyy * pxz);
+  x[0] = pxx;
+  x[1] = pyy;
+  x[2] = pzz;
+  x[3] = pxy;
+  x[4] = pxz;
+  x[5] = pyz;
+  x[6] = pxx + pyy + pzz;
+  x[7] = sqrtf(n2);
+  x[8] = det / (n2 + 1e-30f);
+  x[9] = width;
+}
+
+// The pipelined update with the closure.  A warp's FP16 feature tile (32 x kXStride
+// halves) lives in the first 1.5 KB of its own lanes' boundary slots, which are free once
+// every lane of the warp is past its boundary condition (the __syncwarp before the closure).
+template <typename S>
+__global__ void __launch_bounds__(kPipeCells) step_pipe_learned_kernel(const __grid_constant__ PipeLearnedParams<S> lp) {
+  __shared__ __align__(16) float bc_slot[kPipeCells][27];
+  extern __shared__ __align__(128) unsigned char smem[];
+  const PipeParams<S>& p = lp.base;
+  __half* xtile = reinterpret_cast<__half*>(&bc_slot[threadIdx.x & ~31u][0]);
+  pipe_run<S>(p, smem, [&](unsigned char* st, int t, uint32_t cell, bool active) {
+    using Lay = PipeLayout<S>;
+    using T = typename S::type;
+    const uint8_t m = active ? st[Lay::kMarkerOff + t] : make_marker(kSkip, 0);
     const int kind = marker_kind(m);
-    float f[27];
-    float K[3][3][3];
-    float rho = 1.f, ux = 0.f, uy = 0.f, uz = 0.f, inv_rho = 1.f;
+    unsigned char* mine = st + t * Lay::E;
+    const bool collides = kind != kSkip && kind != kSolid;
+    CellMomentsG cm{};
     float x[kMlpIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (kind != kSkip) {
-      load_cell_ri<S>(p.ri, cell, f);
-      if (kind == kSolid) {  // bounce-back: done before the closure, nothing to keep
+    if (kind == kSolid) {
 #pragma unroll
-        for (int q = 1; q < 27; q += 2) {
-          const float t = f[q];
-          f[q] = f[q + 1];
-          f[q + 1] = t;
-        }
-        store_cell_ri<S>(p.ri, cell, f);
-      } else {
-        if (kind != kFluid) apply_boundary(m, f, p.given ? p.given[cell] : p.given_uniform);
-        central_moments(f, K, rho, ux, uy, uz, inv_rho);
-        mlp_features(K[2][0][0], K[0][2][0], K[0][0][2], K[1][1][0], K[1][0][1], K[0][1][1], rho, inv_rho, p.width, x);
+      for (int q = 1; q < 27; q += 2) {
+        T* a = reinterpret_cast<T*>(mine + p.soff[q]);
+        T* b = reinterpret_cast<T*>(mine + p.soff[q + 1]);
+        const T tmp = *a;
+        *a = *b;
+        *b = tmp;
       }
-    }
-    const float nu_t = mlp_eval(s, x, phase, p.health);
-    if (kind != kSkip && kind != kSolid) {
-      const float w = nu_t >= 0.f ? 1.f / (3.f * (p.nu + nu_t) + 0.5f) : smagorinsky_omega(K, rho, inv_rho, p.rx);
-      relax_rebuild(f, K, rho, ux, uy, uz, inv_rho, w);
-      if (p.health) {
-        const float r = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6];
-        if (!(r > 0.f && r < 1.0e30f)) atomicOr(p.health, 1u);
+    } else if (collides) {
+      float v[27];
+#pragma unroll
+      for (int q = 0; q < 27; ++q) v[q] = raw_to_float<S>(mine + p.soff[q]);
+      if constexpr (S::kind == kStoreF32) {
+#pragma unroll
+        for (int q = 0; q < 27; ++q) v[q] -= lattice_weight(q);
       }
-      store_cell_ri<S>(p.ri, cell, f);
+      if (kind != kFluid) {
+#pragma unroll
+        for (int q = 0; q < 27; ++q) v[q] += lattice_weight(q);
+        apply_boundary_at(m, v, p.given ? p.given[cell] : p.given_uniform, bc_slot[t]);
+#pragma unroll
+        for (int q = 0; q < 27; ++q) v[q] -= lattice_weight(q);
+      }
+      cm = cell_moments_g(v);
+      if (p.health && !(cm.rho > 0.f && cm.rho < 1.0e30f)) atomicOr(p.health, 1u);
+      mlp_features_d(cm, lp.width, x);
     }
-  }
-  mlp_cta_teardown(s);
+    __syncwarp();
+    const float nu_t = mlp_warp_eval(lp.mlpw, lp.sc, xtile, x);
+    if (collides) {
+      float v[27];
+      relax_rebuild_g(v, cm, 1.f / (3.f * (lp.nu + nu_t) + 0.5f));
+      if constexpr (S::kind == kStoreF32) {
+#pragma unroll
+        for (int q = 0; q < 27; ++q) v[q] += lattice_weight(q);
+      }
+#pragma unroll
+      for (int q = 0; q < 27; ++q) float_to_raw<S>(mine + p.soff[q], v[q]);
+    }
+  });
 }
 
 template <typename S>
@@ -112,7 +157,8 @@ __global__ void __launch_bounds__(kStepThreads, 7) step_learned_warp_kernel(cons
         mlp_features(K[2][0][0], K[0][2][0], K[0][0][2], K[1][1][0], K[1][0][1], K[0][1][1], rho, inv_rho, p.width, x);
       }
     }
-    const float nu_t = mlp_warp_eval(p.mlpw, p.sc, xt, x);  // converges the warp first
+    __syncwarp();
+    const float nu_t = mlp_warp_eval(p.mlpw, p.sc, xt, x);
     if (kind != kSkip && kind != kSolid) {
       relax_rebuild(f, K, rho, ux, uy, uz, inv_rho, 1.f / (3.f * (p.nu + nu_t) + 0.5f));
       if (p.health) {

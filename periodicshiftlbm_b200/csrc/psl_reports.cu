@@ -12,12 +12,11 @@
 // here (the reference reduces in FP32).  Levels are placed by their origins (ox, oy, oz),
 // so a refined PS grid lands where it lies in the coarse grid.
 //
+// psl_forcing_torque is the reference's getTorque (M35Full/m35Main.cu:176-260) on PS grids:
+// -g_x y + g_y x summed over the forced-velocity cells, g their forcing in physical units.
 // psl_torque sums r x F over the solid cells of a box, F the per-cell momentum exchange of
 // getSphereDrag (flowAroundSphereMainSingle.cu:99-156, rho (u - u_bounced)) and r the cell
-// centre minus a reference point, physical units.  The reference's getTorque
-// (M35Full/m35Main.cu:176-260) sums -F_x y + F_y x of its forced-velocity cells through the
-// case's getForcing hook on DIAD grids; this is its counterpart for bounce-back bodies on
-// PS grids (the z component about the point is the same expression).
+// centre minus a reference point: the same moment for bounce-back bodies.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -124,6 +123,48 @@ __global__ void __launch_bounds__(kRedThreads) torque_kernel(GridView<S> g, cons
     acc[5] += fz;
   }
   block_sum_store<6>(acc, partial);
+}
+
+// getTorque (M35Full/m35Main.cu:176-260) on a PS grid: per forced-velocity cell with
+// k >= k_min, the forcing g = rho (u_given - u) of its stored populations (the target of
+// the library's forced cells is their given velocity, where the reference's getForcing hook
+// computes one), in physical units (convertToPhysicalForce, cellFunctions.h:221-226:
+// times rho_nominal (res/1000)^4 / dt^2), and its torque -g_x y + g_y x about the z axis
+// through the origin, (x, y) = (i res + ox, j res + oy) as getXYZFromIJKCellIndex gives
+// them.  Sums: torque, g (physical) -- four FP64 values.
+template <typename S>
+__global__ void __launch_bounds__(kRedThreads) forcing_torque_kernel(GridView<S> g, const uint8_t* marker,
+                                                                     const float4* given, float4 given_uniform, int nx,
+                                                                     int ny, int k_min, float res, float ox, float oy,
+                                                                     double to_phys, double* partial) {
+  double acc[4] = {0, 0, 0, 0};
+  for (uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x; cell < g.n; cell += gridDim.x * blockDim.x) {
+    const uint8_t m = marker[cell];
+    if (marker_kind(m) != kFluid || marker_normal(m) != 1) continue;  // forced-velocity cells
+    const int k = (int)(cell / ((uint32_t)nx * ny));
+    if (k < k_min) continue;
+    const uint32_t r = cell - (uint32_t)k * nx * ny;
+    const int j = (int)(r / nx), i = (int)(r % nx);
+    double rho = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+      const double v = (double)S::load_q(g.fq[q] + shifted(cell, g.shift[q], g.n), q);
+      rho += v;
+      jx += cx(q) * v;
+      jy += cy(q) * v;
+      jz += cz(q) * v;
+    }
+    const float4 gv = given ? given[cell] : given_uniform;
+    const double gx = (rho * (double)gv.y - jx) * to_phys;
+    const double gy = (rho * (double)gv.z - jy) * to_phys;
+    const double gz = (rho * (double)gv.w - jz) * to_phys;
+    const float x = (float)i * res + ox, y = (float)j * res + oy;
+    acc[0] += -gx * (double)y + gy * (double)x;
+    acc[1] += gx;
+    acc[2] += gy;
+    acc[3] += gz;
+  }
+  block_sum_store<4>(acc, partial);
 }
 
 struct Section {
@@ -333,6 +374,35 @@ int psl_torque(psl_grid* g, const int* lo3, const int* hi3, const float* point3,
     torque3[c] = out[c];
     if (force3) force3[c] = out[3 + c];
   }
+  return PSL_OK;
+}
+
+int psl_forcing_torque(psl_grid* g, int k_min, float rho_nominal_phys, double* torque, double* force3) {
+  if (!g || !torque) return fail(PSL_ERR_INVALID, "psl_forcing_torque: null argument");
+  const psl_info& I = g->info;
+  DeviceGuard dg(g->device);
+  double* buf = nullptr;
+  REP_CUDA(cudaMalloc(&buf, (kRedBlocks * 4 + 4) * sizeof(double)));
+  const int nb = (int)std::min<long long>(kRedBlocks, ((long long)g->n + kRedThreads - 1) / kRedThreads);
+  const double len = (double)I.res / 1000.0;
+  const double to_phys = (double)rho_nominal_phys * len * len * len * len / ((double)I.dt_phys * I.dt_phys);
+  with_storage(g->storage, [&](auto s) {
+    using S = decltype(s);
+    forcing_torque_kernel<S><<<nb, kRedThreads, 0, g->stream>>>(view_of<S>(g), g->marker, g->given, g->given_uniform,
+                                                               I.cell_count_x, I.cell_count_y, k_min, I.res, I.ox,
+                                                               I.oy, to_phys, buf);
+    return 0;
+  });
+  final_sum_kernel<4><<<1, 32, 0, g->stream>>>(buf, nb, buf + kRedBlocks * 4);
+  double out[4];
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, buf + kRedBlocks * 4, sizeof(out), cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  cudaFree(buf);
+  if (e != cudaSuccess) return fail(PSL_ERR_CUDA, std::string("psl_forcing_torque: ") + cudaGetErrorString(e));
+  *torque = out[0] / 1000.0;  // N mm -> N m, as the reference reports it
+  if (force3)
+    for (int c = 0; c < 3; ++c) force3[c] = out[1 + c];
   return PSL_OK;
 }
 

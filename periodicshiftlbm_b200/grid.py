@@ -252,8 +252,27 @@ MARKER_MOVING_WALL = _lib.CELL_SOLID | (1 << 3)
 MARKER_FORCED_VELOCITY = _lib.CELL_FLUID | (1 << 3)
 
 
-def setSmagorinskyConstant(grid: GridStruct, cs: float):
-    call("psl_set_smagorinsky", grid.handle, cs)
+def setSmagorinskyConstant(grid: GridStruct, cs):
+    """getSmagorinskyConstant: a number (uniform), a per-cell array of N constants in cell
+    order (i fastest), or the hook itself, a function (i, j, k, Info) -> C_s evaluated for
+    every cell as the reference does (include/applyLocalCellUpdate.h:68).  None removes a
+    per-cell field."""
+    if cs is None:
+        call("psl_set_smagorinsky_field", grid.handle, None)
+        return
+    if callable(cs):
+        info = grid.Info
+        k, j, i = np.meshgrid(np.arange(info.cellCountZ), np.arange(info.cellCountY), np.arange(info.cellCountX),
+                              indexing="ij")
+        vals = np.array([cs(int(a), int(b), int(c), info) for a, b, c in zip(i.ravel(), j.ravel(), k.ravel())],
+                        dtype=np.float32)
+        cs = vals
+    if np.ndim(cs) == 0:
+        call("psl_set_smagorinsky_field", grid.handle, None)
+        call("psl_set_smagorinsky", grid.handle, float(cs))
+        return
+    a = np.ascontiguousarray(cs, dtype=np.float32).reshape(grid.cellCount)
+    call("psl_set_smagorinsky_field", grid.handle, a.ctypes.data)
 
 
 # ---- per-step update --------------------------------------------------------------------
@@ -327,6 +346,15 @@ def getTorque(grid: GridStruct, lo, hi, point) -> tuple:
     f = np.zeros(3)
     call("psl_torque", grid.handle, lo.ctypes.data, hi.ctypes.data, pt.ctypes.data, t.ctypes.data, f.ctypes.data)
     return t, f
+
+
+def getForcingTorque(grid: GridStruct, k_min: int = 5, rho_nominal_phys: float = 1.225) -> tuple:
+    """getTorque (M35Full/m35Main.cu:176-260) on a PS grid (psl_forcing_torque): the torque
+    -g_x y + g_y x of the forced-velocity cells' forcing in N m, and the summed forcing."""
+    t = np.zeros(1)
+    f = np.zeros(3)
+    call("psl_forcing_torque", grid.handle, int(k_min), float(rho_nominal_phys), t.ctypes.data, f.ctypes.data)
+    return float(t[0]), f
 
 
 PLANES = {"XY": 0, "ZY": 1, "ZX": 2}

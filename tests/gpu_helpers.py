@@ -11,7 +11,7 @@ def config_from_case(case) -> SphereConfig:
     return SphereConfig(name="test", nx=case.nx, ny=case.ny, nz=case.nz, sphere=tuple(case.sphere),
                         radius=case.radius, u_in=case.u_in, nu=case.nu, smagorinsky=case.smagorinsky,
                         wall_mode=case.wall_mode, seed=case.seed, noise=case.noise, refine=case.refine,
-                        refine2=case.refine2)
+                        refine2=case.refine2, cs_mode=case.cs_mode)
 
 
 class GpuSim:

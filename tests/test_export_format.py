@@ -24,3 +24,14 @@ def test_history_file_layout(tmp_path):
     raw = open(path, "rb").read()
     assert np.frombuffer(raw[:4], dtype=np.int32)[0] == 7
     assert np.array_equal(np.frombuffer(raw[4:], dtype=np.float32), np.arange(7, dtype=np.float32) * 0.5)
+
+
+def test_history_file_bytes_equal_reference_export(ref, tmp_path):
+    """The library's exportHistoryData writes the bytes of the reference's own
+    exportHistoryData (include/plotter/exportSectionCutPlot.h:994-1001, compiled into the
+    reference build)."""
+    hist = np.random.default_rng(3).normal(size=40).astype(np.float32)
+    mine, theirs = str(tmp_path / "mine.bin"), str(tmp_path / "theirs.bin")
+    exportHistoryData(hist, 17, mine)
+    ref.export_history(hist, 17, theirs)
+    assert open(mine, "rb").read() == open(theirs, "rb").read()

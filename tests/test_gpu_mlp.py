@@ -49,20 +49,24 @@ def periodic_grid(storage="f32", n=(16, 12, 10), nu=0.01, seed=1):
     return g
 
 
-@pytest.mark.parametrize("path", ["warp", "tcgen05"])
-def test_constant_closure_equals_plain_update_with_added_viscosity(path, monkeypatch):
-    monkeypatch.setenv("PSL_CLOSURE_PATH", path)
-    _constant_closure_check()
+# grid shapes: 16x12x10 (N a multiple of 8) takes the pipelined kernels, 15x11x9 (N odd)
+# the one-thread-per-cell kernels
+SHAPES = {"pipe": (16, 12, 10), "direct": (15, 11, 9)}
 
 
-def _constant_closure_check():
+@pytest.mark.parametrize("path", ["pipe", "direct"])
+def test_constant_closure_equals_plain_update_with_added_viscosity(path):
+    _constant_closure_check(SHAPES[path])
+
+
+def _constant_closure_check(shape):
     p = {k: np.zeros_like(v) for k, v in mo.random_params(0).items()}
     p["in_scale"] = np.ones(10)
     p["b3"] = np.float64(0.3)
     p["out_scale"] = np.float64(0.004)
     nu_t = float(mlp_infer(p, np.zeros((1, 10), np.float32))[0])
-    a = periodic_grid(nu=0.01)
-    b = periodic_grid(nu=float(np.float32(0.01) + np.float32(nu_t)))
+    a = periodic_grid(n=shape, nu=0.01)
+    b = periodic_grid(n=shape, nu=float(np.float32(0.01) + np.float32(nu_t)))
     set_sgs_mlp(a, p, 1.0)
     for _ in range(5):
         for g in (a, b):
@@ -74,13 +78,13 @@ def _constant_closure_check():
     b.close()
 
 
-@pytest.mark.parametrize("path", ["warp", "tcgen05"])
-@pytest.mark.parametrize("storage", ["f32", "f16"])
-def test_fused_learned_update_matches_oracle_cell_by_cell(orc, storage, path, monkeypatch):
-    """Both evaluations of the fused closure: per-warp MMAs (default) and CTA-wide tcgen05."""
-    monkeypatch.setenv("PSL_CLOSURE_PATH", path)
+@pytest.mark.parametrize("path", ["pipe", "direct"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+def test_fused_learned_update_matches_oracle_cell_by_cell(orc, storage, path):
+    """Both kernels with the fused closure: the pipelined tile update and the
+    one-thread-per-cell update."""
     p = mo.random_params(5)
-    g = periodic_grid(storage=storage, nu=0.01)
+    g = periodic_grid(storage=storage, n=SHAPES[path], nu=0.01)
     set_sgs_mlp(g, p, 1.0)
     applyStreaming(g)
     f_in = g.fArray  # the populations each cell loads
@@ -94,9 +98,10 @@ def test_fused_learned_update_matches_oracle_cell_by_cell(orc, storage, path, mo
     want = np.stack([orc.collision(f_in[:, c], float(np.float32(0.01) + nu_t[c]), 0.0) for c in idx], axis=1)
     if storage == "f32":
         assert rel(f_out[:, idx], want) < 1e-5
-    else:  # the result is stored as FP16 f - w
+    else:  # the result is stored as 16-bit f - w
         w = np.array([8 / 27] + [2 / 27] * 6 + [1 / 54] * 12 + [1 / 216] * 8)[:, None]
-        assert np.max(np.abs(f_out[:, idx] - want) / np.maximum(np.abs(want - w), 1e-4)) < 2e-3
+        bound = 2e-3 if storage == "f16" else 1.6e-2
+        assert np.max(np.abs(f_out[:, idx] - want) / np.maximum(np.abs(want - w), 1e-4)) < bound
     g.close()
 
 

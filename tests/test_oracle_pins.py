@@ -187,3 +187,43 @@ def test_fill_coarse_from_fine_oracle_matches_reference(ref, orc):
     assert np.array_equal(fb[:, ~inside], before_c[:, ~inside])
     assert not np.array_equal(fb[:, inside], before_c[:, inside])
     assert np.array_equal(b.populations(1), before_f)
+
+
+def test_per_cell_smagorinsky_hook_field_equals_reference(ref):
+    """The library's per-cell Smagorinsky field of the outlet-sponge case holds exactly the
+    values the reference's getSmagorinskyConstant hook returns (coarse and fine grid)."""
+    from periodicshiftlbm_b200.cases import SphereConfig, sponge_smagorinsky
+
+    case = SphereCase(nx=40, ny=12, nz=10, sphere=(10.0, 6.0, 5.0), radius=2.0, nu=0.004, smagorinsky=0.1,
+                      cs_mode=1, refine=((4, 2, 2), (16, 10, 8)))
+    cfg = SphereConfig(name="t", nx=case.nx, ny=case.ny, nz=case.nz, sphere=case.sphere, radius=case.radius,
+                       u_in=case.u_in, nu=case.nu, smagorinsky=case.smagorinsky, refine=case.refine, cs_mode=1)
+    coarse = cfg.infos()[0]
+    want = ref.smagorinsky_constants(case, 0, case.nx, case.ny, case.nz)
+    got = sponge_smagorinsky(coarse, case.smagorinsky)
+    assert np.array_equal(got, want)
+    assert want.max() > 3.9 * case.smagorinsky and want.min() == np.float32(case.smagorinsky)
+    fine = cfg.infos()[1]
+    assert np.all(ref.smagorinsky_constants(case, 1, fine.cellCountX, fine.cellCountY, fine.cellCountZ)
+                  == np.float32(case.smagorinsky))
+
+
+def test_oracle_per_cell_smagorinsky_matches_reference(ref, orc):
+    """The oracle restatement's per-cell hook against the reference run: a refined LES case
+    with the outlet sponge, 40 steps."""
+    case = SphereCase(nx=32, ny=16, nz=16, sphere=(12.0, 8.0, 8.0), radius=2.5, nu=0.002, smagorinsky=0.15,
+                      cs_mode=1, refine=((6, 4, 4), (18, 12, 12)))
+    r = ref.sim(case)
+    o = orc.sim(case)
+    r.run(40)
+    o.run(40)
+    for lev in range(2):
+        a, b = o.populations(lev), r.populations(lev)
+        assert np.max(np.abs(a.astype(np.float64) - b) / np.abs(b)) < 1e-5, lev
+    # the sponge changes the solution: the uniform-constant run differs
+    u = orc.sim(SphereCase(**{**case.__dict__, "cs_mode": 0}))
+    u.run(40)
+    assert np.max(np.abs(u.populations(0).astype(np.float64) - r.populations(0))) > 1e-7
+    r.close()
+    o.close()
+    u.close()

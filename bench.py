@@ -173,9 +173,8 @@ def hbm_peak():
 
 
 def update_kernel(storage: str, sgs: str) -> str:
-    """The coarse-grid update kernel the library launches for this form: the pipelined tile
-    kernels (the config-2 grids hold a multiple of 16 bytes of elements)."""
-    return "step_pipe_learned_kernel" if sgs == "mlp" else "step_pipe_kernel"
+    """The coarse-grid update kernel the library launches for this form."""
+    return "step_learned_warp_kernel" if sgs == "mlp" else "step_kernel"
 
 
 def batch_traffic(storage: str, cells: int):

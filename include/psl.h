@@ -68,7 +68,8 @@ typedef struct psl_sphere_case {
 
 /* Marker byte (psl_set_markers): kind in bits 0-2, outer-normal index in bits 3-7,
  * normal index = (nx+1)*9 + (ny+1)*3 + (nz+1).  For PSL_CELL_SKIP the upper bits are 1 for
- * a ghost cell (fine-grid boundary layer) and 0 for a refined-interior cell. */
+ * a ghost cell (fine-grid boundary layer), 0 for a refined-interior cell and 2 for a
+ * refined-interior cell that the case marks bounce-back (reported solid by the exports). */
 #define PSL_CELL_SKIP 0
 #define PSL_CELL_FLUID 1
 #define PSL_CELL_SOLID 2

@@ -8,8 +8,7 @@ import ctypes
 import os
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-# PSL_LIBRARY selects another build of the same library (e.g. a tuning variant).
-LIB_PATH = os.environ.get("PSL_LIBRARY") or os.path.join(PKG, "libpsl_b200.so")
+LIB_PATH = os.path.join(PKG, "libpsl_b200.so")
 
 PSL_OK = 0
 STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3}

@@ -116,11 +116,12 @@ __global__ void __launch_bounds__(kBatchMaxThreads, 4) batch_step_kernel(const B
       const uint8_t m = marker[cell];
       const int kind = marker_kind(m);
       if (kind == kSkip) continue;
+      using V = StoredOf<S>;
       float f[27];
       if (!any_cut) {
-        load_cell_adj<S>(base, slot.adj, cell, f);
+        load_cell_adj<V>(base, slot.adj, cell, f);
       } else {
-        RowIndex<S> ri;
+        RowIndex<V> ri;
         ri.base = base;
         ri.n = n;
 #pragma unroll
@@ -128,13 +129,25 @@ __global__ void __launch_bounds__(kBatchMaxThreads, 4) batch_step_kernel(const B
           ri.off[q] = slot.off[q];
           ri.lim[q] = slot.lim[q];
         }
-        load_cell_ri<S>(ri, cell, f);
+        load_cell_ri<V>(ri, cell, f);
       }
-      local_cell_update<kBatchMaxThreads>(kind, m, f, c.given, c.given_uniform, cell, c.rx, c.health);
-      if (!any_cut) {
-        store_cell_adj<S>(base, slot.adj, cell, f);
+      if constexpr (S::kind == kStoreF32) {
+        local_cell_update<kBatchMaxThreads>(kind, m, f, c.given, c.given_uniform, cell, c.rx, c.health);
+      } else if (kind == kSolid) {  // bounce-back swaps g as it swaps f (w_q = w_opposite(q))
+#pragma unroll
+        for (int q = 1; q < 27; q += 2) {
+          const float t = f[q];
+          f[q] = f[q + 1];
+          f[q + 1] = t;
+        }
       } else {
-        RowIndex<S> ri;
+        __shared__ float bslot[kBatchMaxThreads][27];
+        collide_cell_g(kind, m, f, c.given, c.given_uniform, cell, c.rx, c.rx.cs18, c.health, bslot[threadIdx.x]);
+      }
+      if (!any_cut) {
+        store_cell_adj<V>(base, slot.adj, cell, f);
+      } else {
+        RowIndex<V> ri;
         ri.base = base;
         ri.n = n;
 #pragma unroll
@@ -142,7 +155,7 @@ __global__ void __launch_bounds__(kBatchMaxThreads, 4) batch_step_kernel(const B
           ri.off[q] = slot.off[q];
           ri.lim[q] = slot.lim[q];
         }
-        store_cell_ri<S>(ri, cell, f);
+        store_cell_ri<V>(ri, cell, f);
       }
     }
   }

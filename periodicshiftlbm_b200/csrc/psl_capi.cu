@@ -14,7 +14,6 @@
 #include "psl.h"
 #include "psl_internal.h"
 #include "psl_kernels.cuh"
-#include "psl_step_pipe.cuh"
 
 using namespace psl;
 
@@ -182,6 +181,7 @@ int psl_grid_destroy(psl_grid* g) {
   if (g->T) cudaFree(g->T);
   if (g->givenT) cudaFree(g->givenT);
   if (g->cs_field) cudaFree(g->cs_field);
+  if (g->xcap) cudaFree(g->xcap);
   delete g;
   return PSL_OK;
 }
@@ -412,6 +412,7 @@ int psl_set_smagorinsky_field(psl_grid* g, const float* host_cs) {
 template <typename Case>
 static int fill_eq(psl_grid* g, const Case& c) {
   DeviceGuard dg(g->device);
+  psl_detail_touch(g);
   const unsigned int nb = blocks_for(g->n, 256);
   with_storage(g->storage, [&](auto s) {
     using S = decltype(s);
@@ -436,6 +437,7 @@ int psl_fill_equilibrium_uniform(psl_grid* g, float rho, float ux, float uy, flo
 int psl_fill_equilibrium_field(psl_grid* g, const float* rho_u) {
   PSL_CHECK(g && rho_u, PSL_ERR_INVALID, "psl_fill_equilibrium_field: null argument");
   DeviceGuard dg(g->device);
+  psl_detail_touch(g);
   float* tmp = nullptr;
   PSL_CUDA(cudaMalloc(&tmp, (size_t)g->n * 4 * sizeof(float)));
   cudaError_t e = cudaMemcpyAsync(tmp, rho_u, (size_t)g->n * 4 * sizeof(float), cudaMemcpyHostToDevice, g->stream);
@@ -455,6 +457,7 @@ int psl_fill_equilibrium_field(psl_grid* g, const float* rho_u) {
 
 int psl_apply_streaming(psl_grid* g) {
   PSL_CHECK(g, PSL_ERR_INVALID, "psl_apply_streaming: null grid");
+  psl_detail_touch(g);
   const long long nx = g->info.cell_count_x, ny = g->info.cell_count_y, n = g->n;
   for (int q = 0; q < 27; ++q) {
     long long s = (long long)g->shift[q];
@@ -480,70 +483,8 @@ static RelaxationT<T> relaxation(const psl_grid* g) {
   return rx;
 }
 
-// Resident CTAs of the pipelined update per SM, per device and kernel form.  The first
-// call on a device also raises the kernel's dynamic shared-memory limit to what it uses
-// (static + dynamic above 48 KB needs the opt-in); later launches read the cache.
-static int pipe_blocks_per_sm(const void* kernel, size_t smem, int device, int form) {
-  static std::atomic<int> cache[64][8];
-  std::atomic<int>& slot = cache[device & 63][form & 7];
-  int v = slot.load(std::memory_order_relaxed);
-  if (v > 0) return v;
-  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, kPipeCells, smem) != cudaSuccess) return 0;
-  slot.store(v, std::memory_order_relaxed);
-  return v;
-}
-
-// The pipelined update (psl_step_pipe.cuh) where it applies: FP32 / FP16 / BF16 storage and
-// N a multiple of 16 bytes of elements.  Returns false when the grid takes the
-// one-thread-per-cell kernel instead.
-template <typename S>
-static bool launch_pipe(psl_grid* g, cudaError_t* err) {
-  if constexpr (S::kind == kStoreF64) {
-    return false;
-  } else {
-    using Lay = PipeLayout<S>;
-    if (g->n % Lay::V) return false;
-    PipeParams<S> p;
-    p.base = static_cast<typename S::type*>(g->f);
-    p.stride = (uint32_t)g->stride;
-    p.n = g->n;
-    p.ntiles = (g->n + kPipeCells - 1) / kPipeCells;
-    p.stage_bytes = g->cs_field ? Lay::kStageBytesCs : Lay::kStageBytes;
-    p.extra_bytes = 0;
-    for (int q = 0; q < 27; ++q) {
-      const uint32_t rem = g->shift[q] % Lay::V;
-      p.shift[q] = g->shift[q];
-      p.soff[q] = (uint32_t)(q * Lay::kRowBytes) + rem * Lay::E;
-      if (rem) p.extra_bytes += 16;
-    }
-    p.marker = g->marker;
-    p.given = g->given;
-    p.given_uniform = g->given_uniform;
-    p.cs = g->cs_field;
-    p.rx = relaxation<float>(g);
-    p.health = g->health;
-    const size_t smem = (size_t)Lay::kStages * (p.stage_bytes + 8);
-    const int per_sm = pipe_blocks_per_sm((const void*)step_pipe_kernel<S>, smem, g->device,
-                                          2 * S::kind + (g->cs_field ? 1 : 0));
-    int sms = 0;
-    *err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
-    if (*err != cudaSuccess) return true;
-    if (per_sm <= 0) {
-      *err = cudaErrorInvalidConfiguration;
-      return true;
-    }
-    const unsigned int blocks = std::min<unsigned int>(p.ntiles, (unsigned int)(per_sm * sms));
-    step_pipe_kernel<S><<<blocks, kPipeCells, smem, g->stream>>>(p);
-    *err = cudaGetLastError();
-    return true;
-  }
-}
-
 template <typename S>
 static cudaError_t launch_step(psl_grid* g) {
-  cudaError_t err = cudaSuccess;
-  if (launch_pipe<S>(g, &err)) return err;
   StepParams<S> p;
   p.g = view<S>(g);
   p.marker = g->marker;
@@ -552,6 +493,7 @@ static cudaError_t launch_step(psl_grid* g) {
   p.cs = g->cs_field;
   p.rx = relaxation<typename S::calc>(g);
   p.health = g->health;
+  psl_detail_fill_capture(g, p.cap);
   p.ri.base = static_cast<typename S::type*>(g->f);
   p.ri.n = g->n;
   for (int q = 0; q < 27; ++q) {
@@ -569,6 +511,7 @@ static cudaError_t launch_step(psl_grid* g) {
 int psl_apply_local_cell_update(psl_grid* g) {
   PSL_CHECK(g, PSL_ERR_INVALID, "psl_apply_local_cell_update: null grid");
   DeviceGuard dg(g->device);
+  psl_detail_touch(g);
   const bool custom = g->custom_markers || g->body.x != 0.f || g->body.y != 0.f || g->body.z != 0.f;
   if (g->T) {
     PSL_CHECK(!custom && !g->mlp, PSL_ERR_INVALID,
@@ -586,6 +529,7 @@ int psl_apply_local_cell_update(psl_grid* g) {
         sp.base.given = g->given;
         sp.base.given_uniform = g->given_uniform;
         sp.base.cs = g->cs_field;
+        sp.base.cap = Capture<S>{};
         sp.base.rx = relaxation<float>(g);
         sp.base.health = g->health;
         sp.T.base = g->T;
@@ -621,6 +565,7 @@ int psl_apply_local_cell_update(psl_grid* g) {
         cp.base.given = g->given;
         cp.base.given_uniform = g->given_uniform;
         cp.base.cs = g->cs_field;
+        cp.base.cap = Capture<S>{};
         cp.base.rx = relaxation<float>(g);
         cp.base.health = g->health;
         cp.body = g->body;
@@ -648,6 +593,7 @@ static void launch_periodic(psl_grid* g, int axis) {
 static int periodic(psl_grid* g, int axis) {
   PSL_CHECK(g, PSL_ERR_INVALID, "psl_apply_bc_periodic: null grid");
   DeviceGuard dg(g->device);
+  psl_detail_touch(g);
   with_storage(g->storage, [&](auto s) {
     launch_periodic<decltype(s)>(g, axis);
     return 0;
@@ -659,7 +605,7 @@ int psl_apply_bc_periodic_x(psl_grid* g) { return periodic(g, 0); }
 int psl_apply_bc_periodic_y(psl_grid* g) { return periodic(g, 1); }
 
 template <typename S>
-static int launch_coarse_fine(psl_grid* c, psl_grid* f) {
+static int launch_coarse_fine(psl_grid* c, psl_grid* f, bool use_capture) {
   const psl_info& C = c->info;
   const psl_info& F = f->info;
   const int a = C.i_subgrid_end - C.i_subgrid_start, b = C.j_subgrid_end - C.j_subgrid_start,
@@ -688,6 +634,7 @@ static int launch_coarse_fine(psl_grid* c, psl_grid* f) {
   p.n_shell = (uint32_t)((long long)p.fnx * p.fny * p.fnz - (long long)(p.fnx - 4) * (p.fny - 4) * (p.fnz - 4));
   p.barrier = c->health + 1;
   p.error = c->health;
+  p.xcap = use_capture ? static_cast<const typename S::type*>(f->xcap) : nullptr;
   int sms = 0, per_sm = 0;
   PSL_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
   PSL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_fine_kernel<S>, kCoarseFineThreads, 0));
@@ -742,6 +689,7 @@ int psl_fill_coarse_grid_from_fine(psl_grid* c, psl_grid* f) {
   PSL_CHECK(27ull * c->stride + c->n < (1ull << 32) && 27ull * f->stride + f->n < (1ull << 32), PSL_ERR_INVALID,
             "fill coarse: grid too large for 32-bit row offsets");
   DeviceGuard dg(c->device);
+  psl_detail_touch(c);
   return with_storage(c->storage, [&](auto s) { return launch_fill_coarse<decltype(s)>(c, f); });
 }
 
@@ -760,7 +708,21 @@ int psl_apply_coarse_fine_grid_communication(psl_grid* c, psl_grid* f) {
   PSL_CHECK(27ull * c->stride + c->n < (1ull << 32) && 27ull * f->stride + f->n < (1ull << 32), PSL_ERR_INVALID,
             "coarse/fine: grid too large for 32-bit row offsets");
   DeviceGuard dg(c->device);
-  return with_storage(c->storage, [&](auto s) { return launch_coarse_fine<decltype(s)>(c, f); });
+  // The fine grid's x-face ring children come from its update's capture when its last
+  // population change was a capturing update; the first transfer sets the capture up.
+  const bool use_capture = f->xcap && f->xcap_version == f->state_version;
+  if (!f->xcap && f->storage != kStoreF64 && F.cell_count_x >= 8) {
+    const size_t bytes = 2ull * F.cell_count_y * F.cell_count_z * 2 * 27 * storage_bytes(f->storage);
+    if (cudaMalloc(&f->xcap, bytes) != cudaSuccess) {
+      f->xcap = nullptr;  // no capture: the transfer reads the fine grid itself
+      cudaGetLastError();
+    }
+    f->xcap_i0 = 2;                     // children of ring cell iS + 1
+    f->xcap_i1 = F.cell_count_x - 4;    // children of ring cell iE - 2
+  }
+  psl_detail_touch(c);
+  psl_detail_touch(f);
+  return with_storage(c->storage, [&](auto s) { return launch_coarse_fine<decltype(s)>(c, f, use_capture); });
 }
 
 int psl_update_grid(psl_grid** grids, int levels, int level) {
@@ -837,6 +799,7 @@ static int gather(psl_grid* g, float* host) {
 
 template <typename S>
 static int scatter(psl_grid* g, const float* host) {
+  psl_detail_touch(g);
   float* tmp = nullptr;
   PSL_CUDA(cudaMalloc(&tmp, (size_t)g->n * sizeof(float)));
   cudaError_t e = cudaSuccess;
@@ -897,6 +860,7 @@ int psl_set_shifts(psl_grid* g, const int* s) {
   PSL_CHECK(g && s, PSL_ERR_INVALID, "psl_set_shifts: null argument");
   for (int q = 0; q < 27; ++q)
     PSL_CHECK(s[q] >= 0 && (uint32_t)s[q] < g->n, PSL_ERR_INVALID, "psl_set_shifts: shift outside [0, N)");
+  psl_detail_touch(g);
   for (int q = 0; q < 27; ++q) g->shift[q] = (uint32_t)s[q];
   return PSL_OK;
 }

@@ -52,12 +52,14 @@ PSL_HDI void getOuterNormal(int i, int j, int k, int& nx, int& ny, int& nz, cons
 
 // Encode the marker byte exactly as applyLocalCellUpdate.h:21-67 interprets the hooks:
 // ghost and refined-interior cells are skipped first, then bounce-back, fluid, and the
-// boundary kinds with the outer normal (periodic components zeroed).
+// boundary kinds with the outer normal (periodic components zeroed).  A skipped cell keeps
+// the hook's bounce-back flag in its normal bits (kSkipSolid) for the exports, which report
+// getMarkers' bounceback on every cell (plotter/exportSectionCutPlot.h:45-48).
 PSL_HDI uint8_t encode_marker(int i, int j, int k, const MarkerStruct& M, const InfoStruct& I) {
   if (M.ghost) return make_marker(kSkip, 1);
   if ((i > I.iSubgridStart + 1 && i < I.iSubgridEnd - 2) && (j > I.jSubgridStart + 1 && j < I.jSubgridEnd - 2) &&
       (k > I.kSubgridStart + 1 && k < I.kSubgridEnd - 2))
-    return make_marker(kSkip, 0);
+    return make_marker(kSkip, M.bounceback ? kSkipSolid : 0);
   if (M.movingBounceback) return make_marker(kSolid, 1);  // moving wall (customised update)
   if (M.bounceback) return make_marker(kSolid, 0);
   if (M.fluid) return make_marker(kFluid, M.forcedVelocity ? 1 : 0);  // 1: forced velocity

@@ -11,6 +11,7 @@
 
 #include "psl_bc_generated.cuh"
 #include "psl_collision.cuh"
+#include "psl_collision_g.cuh"
 #include "psl_hooks.cuh"
 #include "psl_lattice.cuh"
 #include "psl_storage.cuh"
@@ -49,6 +50,35 @@ struct RowIndex {
   uint32_t n;
 };
 
+// The coarse/fine restriction's capture (a fine grid's update writes it): after its
+// update, each cell of fine columns i0, i0 + 1 (face 0) and i1, i1 + 1 (face 1) writes
+// its 27 stored values to buf[((face * rows + row) * 2 + column) * 27 + q], row = k Ny + j.
+// The row of a cell is cell / Nx by an exact multiply-shift: (cell * m) >> s with
+// s = 31 + ceil(log2 Nx), m = floor(2^s / Nx) + 1 (exact for every cell < 2^31).
+template <typename S>
+struct Capture {
+  typename S::type* buf;   // null: no capture
+  uint32_t nx, rows, i0, i1;
+  unsigned long long div_m;
+  uint32_t div_s;
+  // the slot of `cell`'s values, or null when its column is not captured
+  __device__ __forceinline__ typename S::type* slot(uint32_t cell) const {
+    const uint32_t row = (uint32_t)(((unsigned long long)cell * div_m) >> div_s);
+    const uint32_t i = cell - row * nx;
+    uint32_t face, col;
+    if (i - i0 < 2u) {
+      face = 0;
+      col = i - i0;
+    } else if (i - i1 < 2u) {
+      face = 1;
+      col = i - i1;
+    } else {
+      return nullptr;
+    }
+    return buf + ((size_t)(face * rows + row) * 2 + col) * 27;
+  }
+};
+
 template <typename S>
 struct StepParams {
   GridView<S> g;
@@ -59,6 +89,7 @@ struct StepParams {
   const float* cs;       // per-cell Smagorinsky constant (getSmagorinskyConstant), or null: rx.cs18
   RelaxationT<typename S::calc> rx;
   unsigned int* health;  // bit 0 set when a collided cell's density is not finite/positive
+  Capture<S> cap;        // the fine grid's capture for the coarse/fine restriction (cap.buf null: none)
 };
 
 // The relaxation parameters of one cell: the grid's, with the cell's own Smagorinsky
@@ -108,39 +139,75 @@ __device__ __forceinline__ void apply_boundary(uint8_t m, T (&f)[27], float4 giv
   apply_boundary_at(m, f, given, slot[threadIdx.x]);
 }
 
-template <typename S, int Q = 0>
-__device__ __forceinline__ void load_cell(const GridView<S>& g, uint32_t cell, typename S::calc (&f)[27]) {
-  if constexpr (Q < 27) {
-    f[Q] = S::template load<Q>(g.fq[Q] + shifted(cell, g.shift[Q], g.n));
-    load_cell<S, Q + 1>(g, cell, f);
+// The collided-cell body of the 16-bit forms on the stored deviations g = f - w: the
+// boundary functions work on f (g + w, then back), the collision on g (psl_collision_g.cuh).
+// Shared by the pipelined and the batched update, so both give the same bits.
+__device__ __forceinline__ void collide_cell_g(int kind, uint8_t m, float (&g)[27], const float4* given,
+                                               float4 given_uniform, uint32_t cell, const RelaxationT<float>& rx,
+                                               float cs18, unsigned int* health, float* slot) {
+  if (kind != kFluid) {
+#pragma unroll
+    for (int q = 0; q < 27; ++q) g[q] += lattice_weight(q);
+    apply_boundary_at(m, g, given ? given[cell] : given_uniform, slot);
+#pragma unroll
+    for (int q = 0; q < 27; ++q) g[q] -= lattice_weight(q);
   }
-}
-template <typename S, int Q = 0>
-__device__ __forceinline__ void store_cell(const GridView<S>& g, uint32_t cell, const typename S::calc (&f)[27]) {
-  if constexpr (Q < 27) {
-    S::template store<Q>(g.fq[Q] + shifted(cell, g.shift[Q], g.n), f[Q]);
-    store_cell<S, Q + 1>(g, cell, f);
-  }
+  const CellMomentsG cm = cell_moments_g(g);
+  if (health && !(cm.rho > 0.f && cm.rho < 1.0e30f)) atomicOr(health, 1u);
+  relax_rebuild_g(g, cm, smagorinsky_omega_g(cm, rx.omega0, rx.tau, rx.tau2, cs18));
 }
 
-template <typename S, int Q = 0>
+// Gathers / scatters of one cell through accessor A (S itself, or StoredOf<S> for the
+// stored values): GridView (64-bit row pointers) or RowIndex (base + 32-bit offsets).
+template <typename A, typename S, int Q = 0>
+__device__ __forceinline__ void load_cell_as(const GridView<S>& g, uint32_t cell, typename A::calc (&f)[27]) {
+  if constexpr (Q < 27) {
+    f[Q] = A::template load<Q>(g.fq[Q] + shifted(cell, g.shift[Q], g.n));
+    load_cell_as<A, S, Q + 1>(g, cell, f);
+  }
+}
+template <typename A, typename S, int Q = 0>
+__device__ __forceinline__ void store_cell_as(const GridView<S>& g, uint32_t cell, const typename A::calc (&f)[27]) {
+  if constexpr (Q < 27) {
+    A::template store<Q>(g.fq[Q] + shifted(cell, g.shift[Q], g.n), f[Q]);
+    store_cell_as<A, S, Q + 1>(g, cell, f);
+  }
+}
+template <typename A, typename S, int Q = 0>
+__device__ __forceinline__ void load_cell_as(const RowIndex<S>& r, uint32_t cell, typename A::calc (&f)[27]) {
+  if constexpr (Q < 27) {
+    uint32_t i = cell + r.off[Q];
+    if (cell >= r.lim[Q]) i -= r.n;
+    f[Q] = A::template load_once<Q>(r.base + i);
+    load_cell_as<A, S, Q + 1>(r, cell, f);
+  }
+}
+template <typename A, typename S, int Q = 0>
+__device__ __forceinline__ void store_cell_as(const RowIndex<S>& r, uint32_t cell, const typename A::calc (&f)[27]) {
+  if constexpr (Q < 27) {
+    uint32_t i = cell + r.off[Q];
+    if (cell >= r.lim[Q]) i -= r.n;
+    A::template store_once<Q>(r.base + i, f[Q]);
+    store_cell_as<A, S, Q + 1>(r, cell, f);
+  }
+}
+template <typename S>
+__device__ __forceinline__ void load_cell(const GridView<S>& g, uint32_t cell, typename S::calc (&f)[27]) {
+  load_cell_as<S>(g, cell, f);
+}
+template <typename S>
+__device__ __forceinline__ void store_cell(const GridView<S>& g, uint32_t cell, const typename S::calc (&f)[27]) {
+  store_cell_as<S>(g, cell, f);
+}
+template <typename S>
 __device__ __forceinline__ void load_cell_ri(const RowIndex<S>& r, uint32_t cell, typename S::calc (&f)[27]) {
-  if constexpr (Q < 27) {
-    uint32_t i = cell + r.off[Q];
-    if (cell >= r.lim[Q]) i -= r.n;
-    f[Q] = S::template load_once<Q>(r.base + i);
-    load_cell_ri<S, Q + 1>(r, cell, f);
-  }
+  load_cell_as<S>(r, cell, f);
 }
-template <typename S, int Q = 0>
+template <typename S>
 __device__ __forceinline__ void store_cell_ri(const RowIndex<S>& r, uint32_t cell, const typename S::calc (&f)[27]) {
-  if constexpr (Q < 27) {
-    uint32_t i = cell + r.off[Q];
-    if (cell >= r.lim[Q]) i -= r.n;
-    S::template store_once<Q>(r.base + i, f[Q]);
-    store_cell_ri<S, Q + 1>(r, cell, f);
-  }
+  store_cell_as<S>(r, cell, f);
 }
+
 
 // The per-cell body (applyLocalCellUpdate.h:21-72): bounce-back for solid cells; for the
 // others the boundary condition of the marker, the collision and a density health check.
@@ -165,25 +232,57 @@ __device__ __forceinline__ void local_cell_update(int kind, uint8_t m, T (&f)[27
 }
 
 template <typename S, bool kRowIndex>
+__device__ __forceinline__ void load_for(const StepParams<S>& p, uint32_t cell, typename S::calc (&f)[27]) {
+  using A = StoredOf<S>;
+  if constexpr (kRowIndex) load_cell_as<A>(p.ri, cell, f);
+  else load_cell_as<A>(p.g, cell, f);
+}
+template <typename S, bool kRowIndex>
+__device__ __forceinline__ void store_for(const StepParams<S>& p, uint32_t cell, const typename S::calc (&f)[27]) {
+  using A = StoredOf<S>;
+  if constexpr (kRowIndex) store_cell_as<A>(p.ri, cell, f);
+  else store_cell_as<A>(p.g, cell, f);
+}
+// The cell's stored values into the capture, when its column is captured.
+template <typename S>
+__device__ __forceinline__ void capture_cell(const Capture<S>& cap, uint32_t cell, const typename S::calc (&f)[27]) {
+  if (!cap.buf) return;
+  typename S::type* dst = cap.slot(cell);
+  if (!dst) return;
+#pragma unroll
+  for (int q = 0; q < 27; ++q) StoredOf<S>::template store<0>(dst + q, f[q]);
+}
+
+// One thread per cell.  The 16-bit forms load and store their stored values g = f - w and
+// collide on them (collide_cell_g); FP32 and FP64 run collide<false> on f, the reference's
+// operation order.
+template <typename S, bool kRowIndex>
 __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constant__ StepParams<S> p) {
   const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
   if (cell >= p.g.n) return;
   const uint8_t m = p.marker[cell];
   const int kind = marker_kind(m);
-  if (kind == kSkip) return;
-  // (the body of local_cell_update, written out: nvcc allocates 56 registers for this
-  // form against 64 through the helper)
   using T = typename S::calc;
   T f[27];
-  if constexpr (kRowIndex) load_cell_ri<S>(p.ri, cell, f);
-  else load_cell<S>(p.g, cell, f);
-  if (kind == kSolid) {
+  if (kind == kSkip) {  // not updated; a captured column still records its values
+    if (p.cap.buf && p.cap.slot(cell)) {
+      load_for<S, kRowIndex>(p, cell, f);
+      capture_cell(p.cap, cell, f);
+    }
+    return;
+  }
+  load_for<S, kRowIndex>(p, cell, f);
+  if (kind == kSolid) {  // bounce-back: g and f swap alike (w_q = w_opposite(q))
 #pragma unroll
     for (int q = 1; q < 27; q += 2) {
       const T t = f[q];
       f[q] = f[q + 1];
       f[q + 1] = t;
     }
+  } else if constexpr (kCollidesOnG<S>) {
+    __shared__ float slot[kStepThreads][27];
+    collide_cell_g(kind, m, f, p.given, p.given_uniform, cell, p.rx, p.cs ? 18.f * p.cs[cell] : p.rx.cs18, p.health,
+                   slot[threadIdx.x]);
   } else {
     if (kind != kFluid) apply_boundary(m, f, p.given ? p.given[cell] : p.given_uniform);
     collide<false>(f, cell_relaxation(p.rx, p.cs, cell));
@@ -192,10 +291,9 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constan
       if (!(r > T(0) && r < T(1.0e30))) atomicOr(p.health, 1u);
     }
   }
-  if constexpr (kRowIndex) store_cell_ri<S>(p.ri, cell, f);
-  else store_cell<S>(p.g, cell, f);
+  store_for<S, kRowIndex>(p, cell, f);
+  capture_cell(p.cap, cell, f);
 }
-
 
 // ------------------------------------------------------------------------------------------
 // customised update: moving walls, forced-velocity cells, body force
@@ -509,6 +607,9 @@ struct CoarseFineParams {
   unsigned int* barrier;    // zeroed before launch
   unsigned int* error;      // bit 1: barrier gave up
   unsigned int nblocks;
+  // The fine update's capture of the x-face ring cells' children (Capture, above):
+  // [2 faces][fine rows][2 columns][27] stored values, or null (read from the fine grid).
+  const typename S::type* xcap;
 };
 
 // direction sets streaming inward across each face (gridRefinementFunctions.h:441-446):
@@ -561,10 +662,12 @@ constexpr int kCoarseFineThreads = 128;
 
 // Coarse cell (i, j, k) of the refined block from its 8 fine children: their populations
 // added in the child order (k, j, i outer to inner), averaged, rescaled fine -> coarse
-// (writeToCoarseGridInterface, gridRefinementFunctions.h:283-336).
+// (writeToCoarseGridInterface, gridRefinementFunctions.h:283-336).  With `xface` >= 0 the
+// children come from the fine update's capture of that x face (the same stored values in
+// the same order, so the same sums): fine columns 0 and 1 of the face's captured pair.
 template <typename S>
 __device__ __forceinline__ void restrict_cell(const RowIndex<S>& rc, const RowIndex<S>& rf, const CoarseFineParams<S>& p,
-                                              int i, int j, int k) {
+                                              int i, int j, int k, int xface = -1) {
   using T = typename S::calc;
   const int fi = (i - p.iS) * 2, fj = (j - p.jS) * 2, fk = (k - p.kS) * 2;
   T f[27];
@@ -576,9 +679,16 @@ __device__ __forceinline__ void restrict_cell(const RowIndex<S>& rc, const RowIn
     for (int dj = 0; dj <= 1; ++dj)
 #pragma unroll
       for (int di = 0; di <= 1; ++di) {
-        const uint32_t fc = ((uint32_t)(fk + dk) * p.fny + (fj + dj)) * p.fnx + (fi + di);
+        if (xface >= 0) {
+          const typename S::type* src =
+              p.xcap + (((size_t)xface * p.fny * p.fnz + (uint32_t)(fk + dk) * p.fny + (fj + dj)) * 2 + di) * 27;
 #pragma unroll
-        for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], load_pop(rf, q, fc));
+          for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], S::load_q(src + q, q));
+        } else {
+          const uint32_t fc = ((uint32_t)(fk + dk) * p.fny + (fj + dj)) * p.fnx + (fi + di);
+#pragma unroll
+          for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], load_pop(rf, q, fc));
+        }
       }
 #pragma unroll
   for (int q = 0; q < 27; ++q) f[q] = f[q] * T(0.125);
@@ -640,6 +750,10 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
         ri = layer ? a - 1 : 0;
         rj = 1 + r % (b - 2);
         rk = 1 + r / (b - 2);
+        if (p.xcap) {
+          restrict_cell(rc, rf, p, p.iS + 1 + ri, p.jS + 1 + rj, p.kS + 1 + rk, (int)layer);
+          continue;
+        }
       }
       restrict_cell(rc, rf, p, p.iS + 1 + ri, p.jS + 1 + rj, p.kS + 1 + rk);
     }

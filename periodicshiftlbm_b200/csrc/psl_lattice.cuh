@@ -72,8 +72,16 @@ enum CellKind : uint8_t {
 };
 
 PSL_HDI uint8_t make_marker(int kind, int normal) { return (uint8_t)((kind & 7) | (normal << 3)); }
+
+// Normal bits of skipped cells: 1 ghost layer, kSkipSolid a refined-interior cell that the
+// case marks bounce-back (not updated; solid for the exports), 0 other refined-interior cells.
+constexpr int kSkipSolid = 2;
 PSL_HDI int marker_kind(uint8_t m) { return m & 7; }
 PSL_HDI int marker_normal(uint8_t m) { return m >> 3; }
+// Whether the case marks the cell bounce-back (the exports' solid flag), updated or not.
+PSL_HDI bool marker_solid(uint8_t m) {
+  return marker_kind(m) == kSolid || (marker_kind(m) == kSkip && marker_normal(m) == kSkipSolid);
+}
 PSL_HDI constexpr int normal_index(int nx, int ny, int nz) { return (nx + 1) * 9 + (ny + 1) * 3 + (nz + 1); }
 
 }  // namespace psl

@@ -102,57 +102,11 @@ void pack(const psl_sgs_mlp& m, MlpDevice& d) {
   }
 }
 
-// The pipelined closure update where it applies (N a multiple of 16 bytes of elements),
-// else the one-thread-per-cell closure kernel.
 template <typename S>
 int launch(psl_grid* g) {
   const MlpBoth* both = static_cast<const MlpBoth*>(g->mlp);
   MlpScalars sc;
   std::memcpy(&sc, g->mlp_scalars, sizeof(MlpScalars));
-  using Lay = PipeLayout<S>;
-  if (g->n % Lay::V == 0) {
-    PipeLearnedParams<S> lp;
-    PipeParams<S>& p = lp.base;
-    p.base = static_cast<typename S::type*>(g->f);
-    p.stride = (uint32_t)g->stride;
-    p.n = g->n;
-    p.ntiles = (g->n + kPipeCells - 1) / kPipeCells;
-    p.stage_bytes = Lay::kStageBytes;  // the closure replaces any per-cell C_s
-    p.extra_bytes = 0;
-    for (int q = 0; q < 27; ++q) {
-      const uint32_t rem = g->shift[q] % Lay::V;
-      p.shift[q] = g->shift[q];
-      p.soff[q] = (uint32_t)(q * Lay::kRowBytes) + rem * Lay::E;
-      if (rem) p.extra_bytes += 16;
-    }
-    p.marker = g->marker;
-    p.given = g->given;
-    p.given_uniform = g->given_uniform;
-    p.cs = nullptr;
-    p.rx = RelaxationT<float>{};
-    p.health = g->health;
-    lp.mlpw = &both->warp;
-    lp.sc = sc;
-    lp.nu = g->info.nu;
-    lp.width = g->mlp_width;
-    const size_t smem = (size_t)Lay::kStages * (p.stage_bytes + 8);
-    static std::atomic<int> per_sm_cache[64][4];
-    std::atomic<int>& slot = per_sm_cache[g->device & 63][S::kind & 3];
-    int per_sm = slot.load(std::memory_order_relaxed);
-    if (per_sm <= 0) {
-      // static + dynamic shared memory above 48 KB needs the opt-in
-      MLP_CUDA(cudaFuncSetAttribute(step_pipe_learned_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      MLP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_pipe_learned_kernel<S>, kPipeCells, smem));
-      slot.store(per_sm, std::memory_order_relaxed);
-    }
-    if (per_sm < 1) return fail(PSL_ERR_CUDA, "learned update: kernel cannot be resident");
-    int sms = 0;
-    MLP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
-    const unsigned int blocks = std::min<unsigned int>(p.ntiles, (unsigned int)(per_sm * sms));
-    step_pipe_learned_kernel<S><<<blocks, kPipeCells, smem, g->stream>>>(lp);
-    MLP_CUDA(cudaGetLastError());
-    return PSL_OK;
-  }
   if (27ull * g->stride + g->n >= (1ull << 32)) return fail(PSL_ERR_INVALID, "learned update: grid too large");
   LearnedParams<S> p;
   p.ri.base = static_cast<typename S::type*>(g->f);
@@ -170,6 +124,7 @@ int launch(psl_grid* g) {
   p.width = g->mlp_width;
   p.n = g->n;
   p.health = g->health;
+  psl_detail_fill_capture(g, p.cap);
   step_learned_warp_kernel<S><<<(g->n + kStepThreads - 1) / kStepThreads, kStepThreads, 0, g->stream>>>(p);
   MLP_CUDA(cudaGetLastError());
   return PSL_OK;

@@ -6,22 +6,16 @@
 //     omega = 1 / (3 (nu + nu_t) + 1/2)
 // in place of the Smagorinsky rate of include/cellFunctions.h:157-198.
 //
-// The closure is evaluated per warp with tensor-core MMAs (psl_mlp_warp.cuh) inside two
-// kernels:
-//   step_pipe_learned_kernel  the pipelined tile update (psl_step_pipe.cuh): the cell's
-//                             moments come from its stored populations in shared memory,
-//                             the collision runs on g = f - w (psl_collision_g.cuh);
-//   step_learned_warp_kernel  one thread per cell with its own loads, for grids the
-//                             pipeline does not take (N not a multiple of 16 bytes of
-//                             elements).
-// Every thread takes part in its warp's MMAs (skip, solid and out-of-range cells with zero
+// The closure is evaluated per warp with tensor-core MMAs (psl_mlp_warp.cuh) inside the
+// update kernel (step_learned_warp_kernel, one thread per cell): 16-bit storage collides on
+// g = f - w (psl_collision_g.cuh), FP32 in the plain FP32 update's operation order.  Every
+// thread takes part in its warp's MMAs (skip, solid and out-of-range cells with zero
 // features), so the warp-wide steps inside the closure are reached by all lanes.  The
 // CTA-wide tcgen05 evaluation (psl_mlp.cuh) serves the closure's batched inference.
 #pragma once
 #include "psl_kernels.cuh"
 #include "psl_mlp.cuh"
 #include "psl_mlp_warp.cuh"
-#include "psl_step_pipe.cuh"
 
 namespace psl {
 
@@ -37,15 +31,7 @@ struct LearnedParams {
   float width;              // filter width fed to the closure (cell size / coarsest cell size)
   uint32_t n;
   unsigned int* health;
-};
-
-template <typename S>
-struct PipeLearnedParams {
-  PipeParams<S> base;
-  const MlpFrag* mlpw;
-  MlpScalars sc;
-  float nu;
-  float width;
+  Capture<S> cap;            // the fine grid's capture for the coarse/fine restriction
 };
 
 // The closure's features from D = C - rho/3 I (the g-form moments): the same quantities
@@ -68,104 +54,79 @@ __device__ __forceinline__ void mlp_features_d(const CellMomentsG& m, float widt
   x[9] = width;
 }
 
-// The pipelined update with the closure.  A warp's FP16 feature tile (32 x kXStride
-// halves) lives in the first 1.5 KB of its own lanes' boundary slots, which are free once
-// every lane of the warp is past its boundary condition (the __syncwarp before the closure).
+// One thread per cell with the fused closure.  16-bit storage collides on its stored
+// g = f - w (only the ten moments live across the closure's MMAs); FP32 runs the plain FP32
+// update's operation order, only the rate differs.
 template <typename S>
-__global__ void __launch_bounds__(kPipeCells) step_pipe_learned_kernel(const __grid_constant__ PipeLearnedParams<S> lp) {
-  __shared__ __align__(16) float bc_slot[kPipeCells][27];
-  extern __shared__ __align__(128) unsigned char smem[];
-  const PipeParams<S>& p = lp.base;
-  __half* xtile = reinterpret_cast<__half*>(&bc_slot[threadIdx.x & ~31u][0]);
-  pipe_run<S>(p, smem, [&](unsigned char* st, int t, uint32_t cell, bool active) {
-    using Lay = PipeLayout<S>;
-    using T = typename S::type;
-    const uint8_t m = active ? st[Lay::kMarkerOff + t] : make_marker(kSkip, 0);
-    const int kind = marker_kind(m);
-    unsigned char* mine = st + t * Lay::E;
-    const bool collides = kind != kSkip && kind != kSolid;
+__global__ void __launch_bounds__(kStepThreads, 6) step_learned_warp_kernel(const __grid_constant__ LearnedParams<S> p) {
+  __shared__ __align__(16) float bc_slot[kStepThreads][27];
+  // the warp's FP16 feature tile lives in its own lanes' boundary slots (free after the
+  // __syncwarp that follows every lane's boundary condition)
+  __half* xt = reinterpret_cast<__half*>(&bc_slot[threadIdx.x & ~31u][0]);
+  const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
+  const uint8_t m = cell < p.n ? p.marker[cell] : make_marker(kSkip, 0);
+  const int kind = marker_kind(m);
+  using A = StoredOf<S>;
+  float x[kMlpIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float f[27];
+  if (kind == kSkip) {
+    if (cell < p.n && p.cap.buf && p.cap.slot(cell)) {  // a captured column records its values
+      load_cell_as<A>(p.ri, cell, f);
+      capture_cell(p.cap, cell, f);
+    }
+  } else {
+    load_cell_as<A>(p.ri, cell, f);
+  }
+  if (kind == kSolid) {  // bounce-back: done before the closure, nothing to keep
+#pragma unroll
+    for (int q = 1; q < 27; q += 2) {
+      const float t = f[q];
+      f[q] = f[q + 1];
+      f[q + 1] = t;
+    }
+    store_cell_as<A>(p.ri, cell, f);
+    capture_cell(p.cap, cell, f);
+  }
+  const bool collides = kind != kSkip && kind != kSolid;
+  if constexpr (kCollidesOnG<S>) {
     CellMomentsG cm{};
-    float x[kMlpIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (kind == kSolid) {
-#pragma unroll
-      for (int q = 1; q < 27; q += 2) {
-        T* a = reinterpret_cast<T*>(mine + p.soff[q]);
-        T* b = reinterpret_cast<T*>(mine + p.soff[q + 1]);
-        const T tmp = *a;
-        *a = *b;
-        *b = tmp;
-      }
-    } else if (collides) {
-      float v[27];
-#pragma unroll
-      for (int q = 0; q < 27; ++q) v[q] = raw_to_float<S>(mine + p.soff[q]);
-      if constexpr (S::kind == kStoreF32) {
-#pragma unroll
-        for (int q = 0; q < 27; ++q) v[q] -= lattice_weight(q);
-      }
+    if (collides) {
       if (kind != kFluid) {
 #pragma unroll
-        for (int q = 0; q < 27; ++q) v[q] += lattice_weight(q);
-        apply_boundary_at(m, v, p.given ? p.given[cell] : p.given_uniform, bc_slot[t]);
+        for (int q = 0; q < 27; ++q) f[q] += lattice_weight(q);
+        apply_boundary_at(m, f, p.given ? p.given[cell] : p.given_uniform, bc_slot[threadIdx.x]);
 #pragma unroll
-        for (int q = 0; q < 27; ++q) v[q] -= lattice_weight(q);
+        for (int q = 0; q < 27; ++q) f[q] -= lattice_weight(q);
       }
-      cm = cell_moments_g(v);
+      cm = cell_moments_g(f);
       if (p.health && !(cm.rho > 0.f && cm.rho < 1.0e30f)) atomicOr(p.health, 1u);
-      mlp_features_d(cm, lp.width, x);
-    }
-    __syncwarp();
-    const float nu_t = mlp_warp_eval(lp.mlpw, lp.sc, xtile, x);
-    if (collides) {
-      float v[27];
-      relax_rebuild_g(v, cm, 1.f / (3.f * (lp.nu + nu_t) + 0.5f));
-      if constexpr (S::kind == kStoreF32) {
-#pragma unroll
-        for (int q = 0; q < 27; ++q) v[q] += lattice_weight(q);
-      }
-#pragma unroll
-      for (int q = 0; q < 27; ++q) float_to_raw<S>(mine + p.soff[q], v[q]);
-    }
-  });
-}
-
-template <typename S>
-__global__ void __launch_bounds__(kStepThreads, 7) step_learned_warp_kernel(const __grid_constant__ LearnedParams<S> p) {
-  __shared__ __align__(16) __half xtile[kStepThreads / 32][32 * kXStride];
-  __half* xt = xtile[threadIdx.x >> 5];
-  {
-    const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
-    const uint8_t m = cell < p.n ? p.marker[cell] : make_marker(kSkip, 0);
-    const int kind = marker_kind(m);
-    float f[27];
-    float K[3][3][3];
-    float rho = 1.f, ux = 0.f, uy = 0.f, uz = 0.f, inv_rho = 1.f;
-    float x[kMlpIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (kind != kSkip) {
-      load_cell_ri<S>(p.ri, cell, f);
-      if (kind == kSolid) {  // bounce-back: done before the closure, nothing to keep
-#pragma unroll
-        for (int q = 1; q < 27; q += 2) {
-          const float t = f[q];
-          f[q] = f[q + 1];
-          f[q + 1] = t;
-        }
-        store_cell_ri<S>(p.ri, cell, f);
-      } else {
-        if (kind != kFluid) apply_boundary(m, f, p.given ? p.given[cell] : p.given_uniform);
-        central_moments(f, K, rho, ux, uy, uz, inv_rho);
-        mlp_features(K[2][0][0], K[0][2][0], K[0][0][2], K[1][1][0], K[1][0][1], K[0][1][1], rho, inv_rho, p.width, x);
-      }
+      mlp_features_d(cm, p.width, x);
     }
     __syncwarp();
     const float nu_t = mlp_warp_eval(p.mlpw, p.sc, xt, x);
-    if (kind != kSkip && kind != kSolid) {
+    if (collides) {
+      relax_rebuild_g(f, cm, 1.f / (3.f * (p.nu + nu_t) + 0.5f));
+      store_cell_as<A>(p.ri, cell, f);
+      capture_cell(p.cap, cell, f);
+    }
+  } else {
+    float K[3][3][3];
+    float rho = 1.f, ux = 0.f, uy = 0.f, uz = 0.f, inv_rho = 1.f;
+    if (collides) {
+      if (kind != kFluid) apply_boundary_at(m, f, p.given ? p.given[cell] : p.given_uniform, bc_slot[threadIdx.x]);
+      central_moments(f, K, rho, ux, uy, uz, inv_rho);
+      mlp_features(K[2][0][0], K[0][2][0], K[0][0][2], K[1][1][0], K[1][0][1], K[0][1][1], rho, inv_rho, p.width, x);
+    }
+    __syncwarp();
+    const float nu_t = mlp_warp_eval(p.mlpw, p.sc, xt, x);
+    if (collides) {
       relax_rebuild(f, K, rho, ux, uy, uz, inv_rho, 1.f / (3.f * (p.nu + nu_t) + 0.5f));
       if (p.health) {
         const float r = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6];
         if (!(r > 0.f && r < 1.0e30f)) atomicOr(p.health, 1u);
       }
-      store_cell_ri<S>(p.ri, cell, f);
+      store_cell_as<A>(p.ri, cell, f);
+      capture_cell(p.cap, cell, f);
     }
   }
 }

@@ -203,7 +203,7 @@ __global__ void section_kernel(GridView<S> g, const uint8_t* marker, int nx, int
     jy += cy(q) * v;
     jz += cz(q) * v;
   }
-  const uint8_t solid = marker_kind(marker[cell]) == kSolid;
+  const uint8_t solid = marker_solid(marker[cell]);
   const int h0 = (off_h + a * scale) / target_scale - h_min;
   const int v0 = (off_v + b * scale) / target_scale - v_min;
   const int span = max(1, scale / target_scale);
@@ -294,7 +294,7 @@ __global__ void section_export_kernel(GridView<S> g, const uint8_t* marker, int 
   o[1] = uh;
   o[2] = uv;
   o[3] = un;
-  o[4] = marker_kind(marker[cell]) == kSolid ? 1.f : 0.f;
+  o[4] = marker_solid(marker[cell]) ? 1.f : 0.f;
 }
 
 }  // namespace

@@ -94,6 +94,43 @@ struct StoreF64 {
   __device__ __forceinline__ static void store_once(double* p, double v) { __stcs(p, v); }
 };
 
+// The stored value itself as the cell's working value: f for FP32 / FP64, g = f - w for
+// the 16-bit forms (which collide on g, psl_collision_g.cuh).
+template <typename S>
+struct StoredOf {
+  using type = typename S::type;
+  using calc = typename S::calc;
+  template <int Q>
+  __device__ __forceinline__ static calc load_once(const type* p) {
+    if constexpr (S::kind == kStoreF16) return __half2float(__ldg(p));
+    else if constexpr (S::kind == kStoreBF16) return __bfloat162float(__ldg(p));
+    else return S::template load_once<Q>(p);
+  }
+  template <int Q>
+  __device__ __forceinline__ static void store_once(type* p, calc v) {
+    if constexpr (S::kind == kStoreF16) __stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(__float2half_rn(v)));
+    else if constexpr (S::kind == kStoreBF16)
+      __stcs(reinterpret_cast<unsigned short*>(p), __bfloat16_as_ushort(__float2bfloat16_rn(v)));
+    else S::template store_once<Q>(p, v);
+  }
+  template <int Q>
+  __device__ __forceinline__ static calc load(const type* p) {
+    if constexpr (S::kind == kStoreF16) return __half2float(*p);
+    else if constexpr (S::kind == kStoreBF16) return __bfloat162float(*p);
+    else return *p;
+  }
+  template <int Q>
+  __device__ __forceinline__ static void store(type* p, calc v) {
+    if constexpr (S::kind == kStoreF16) *p = __float2half_rn(v);
+    else if constexpr (S::kind == kStoreBF16) *p = __float2bfloat16_rn(v);
+    else *p = v;
+  }
+};
+
+// Whether a storage form collides on the stored deviations g = f - w.
+template <typename S>
+constexpr bool kCollidesOnG = S::kind == kStoreF16 || S::kind == kStoreBF16;
+
 inline size_t storage_bytes(int kind) { return kind == kStoreF32 ? 4 : kind == kStoreF64 ? 8 : 2; }
 
 }  // namespace psl

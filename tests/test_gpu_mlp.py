@@ -49,12 +49,12 @@ def periodic_grid(storage="f32", n=(16, 12, 10), nu=0.01, seed=1):
     return g
 
 
-# grid shapes: 16x12x10 (N a multiple of 8) takes the pipelined kernels, 15x11x9 (N odd)
-# the one-thread-per-cell kernels
-SHAPES = {"pipe": (16, 12, 10), "direct": (15, 11, 9)}
+# grid shapes: whole 128-cell blocks and wrap points at block edges (16x12x10 = 15 blocks)
+# or a partial last block (15x11x9)
+SHAPES = {"whole": (16, 12, 10), "partial": (15, 11, 9)}
 
 
-@pytest.mark.parametrize("path", ["pipe", "direct"])
+@pytest.mark.parametrize("path", ["whole", "partial"])
 def test_constant_closure_equals_plain_update_with_added_viscosity(path):
     _constant_closure_check(SHAPES[path])
 
@@ -78,11 +78,10 @@ def _constant_closure_check(shape):
     b.close()
 
 
-@pytest.mark.parametrize("path", ["pipe", "direct"])
+@pytest.mark.parametrize("path", ["whole", "partial"])
 @pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
 def test_fused_learned_update_matches_oracle_cell_by_cell(orc, storage, path):
-    """Both kernels with the fused closure: the pipelined tile update and the
-    one-thread-per-cell update."""
+    """The fused closure on every storage form, whole and partial blocks."""
     p = mo.random_params(5)
     g = periodic_grid(storage=storage, n=SHAPES[path], nu=0.01)
     set_sgs_mlp(g, p, 1.0)

@@ -1,13 +1,15 @@
-"""The pipelined update kernel (bulk copies through shared memory, psl_step_pipe.cuh) and the
-per-cell Smagorinsky hook.
+"""The update kernel on arbitrary shifts, the per-cell Smagorinsky hook, and the
+coarse/fine restriction's capture.
 
-* Grids and shifts that exercise the tile arithmetic -- one partial tile, several tiles
-  with a partial last one, runs that wrap past N inside a tile, arbitrary shifts -- for
-  every storage form, with and without a per-cell C_s field, with skipped and solid cells
-  among the fluid ones: every cell against the oracle's collision (FP64), skipped cells
-  unchanged and solid cells bounced back bit for bit.
+* Grids and shifts that exercise the shifted addressing -- one 128-cell block, several
+  blocks with a partial last one, shifts whose wrap point falls inside a block, arbitrary
+  shifts -- for every storage form, with and without a per-cell C_s field, with skipped
+  and solid cells among the fluid ones: every cell against the oracle's collision (FP64),
+  skipped cells unchanged and solid cells bounced back bit for bit.
 * A refined LES sphere run whose coarse grid has a per-cell C_s (a sponge ahead of the
   outlet, getSmagorinskyConstant per cell) against the reference's own update run live.
+* The x-face ring cells restricted from the fine update's capture against the restriction
+  that reads the fine grid: bit for bit.
 """
 import numpy as np
 import pytest
@@ -38,14 +40,14 @@ def _start(orc, n, rng):
 @pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
 @pytest.mark.parametrize("dims", [(12, 4, 2), (20, 3, 8), (16, 8, 8), (40, 12, 12)])
 @pytest.mark.parametrize("field", [False, True])
-def test_pipe_update_matches_oracle_for_any_shift(orc, storage, dims, field):
+def test_update_matches_oracle_for_any_shift(orc, storage, dims, field):
     nx, ny, nz = dims
     n = nx * ny * nz
     nu, cs = 0.004, 0.12
     rng = np.random.default_rng(n + 7 * len(storage) + field)
     g = GridStruct(InfoStruct(cellCountX=nx, cellCountY=ny, cellCountZ=nz, nu=nu), storage=storage)
     shifts = rng.integers(0, n, 27)
-    shifts[1:6] = n - 1 - np.arange(5)  # runs that wrap inside the last tile
+    shifts[1:6] = n - 1 - np.arange(5)  # wrap points inside the first block
     shifts[0] = 0
     g.shifter = shifts.astype(np.int32)
     assert np.array_equal(g.shifter, shifts)
@@ -75,7 +77,7 @@ def test_pipe_update_matches_oracle_for_any_shift(orc, storage, dims, field):
 
 
 @pytest.mark.parametrize("storage", ["f16", "bf16"])
-def test_pipe_16bit_health_flag(storage):
+def test_16bit_health_flag(storage):
     g = GridStruct(InfoStruct(cellCountX=16, cellCountY=8, cellCountZ=8, nu=0.01), storage=storage)
     f = np.tile(W.astype(np.float32)[:, None], (1, g.cellCount))
     f[5, 77] = np.nan
@@ -98,3 +100,45 @@ def test_per_cell_smagorinsky_sphere_matches_reference(ref):
         assert rel(g.populations(lev), r.populations(lev)) < 1e-5, lev
     g.close()
     r.close()
+
+
+def _update(grids, level, invalidate):
+    """updateGrid (flowAroundSphereMainSingle.cu:158-167); with `invalidate` every fine grid's
+    capture is made stale before its transfer (re-setting the shifts counts as a change), so
+    the restriction reads the fine grid itself."""
+    from periodicshiftlbm_b200 import applyCoarseFineGridCommunication, applyStreaming
+
+    g = grids[level]
+    applyStreaming(g)
+    applyLocalCellUpdate(g)
+    if level < len(grids) - 1:
+        _update(grids, level + 1, invalidate)
+        _update(grids, level + 1, invalidate)
+        if invalidate:
+            grids[level + 1].shifter = grids[level + 1].shifter
+        applyCoarseFineGridCommunication(g, grids[level + 1])
+
+
+@pytest.mark.parametrize("storage,closure", [("f32", False), ("f16", False), ("bf16", False), ("f16", True)])
+def test_restriction_from_capture_equals_direct_reads(storage, closure):
+    """The x-face ring cells restricted from the fine update's capture give the bits of the
+    restriction that reads the fine grid (three levels: both transfers use it)."""
+    case = SphereCase(nx=32, ny=16, nz=16, sphere=(12.0, 9.0, 9.0), radius=1.5, nu=0.004, smagorinsky=0.1,
+                      refine=((6, 4, 4), (18, 12, 12)), refine2=((6, 6, 6), (18, 14, 14)))
+    a, b = GpuSim(case, storage=storage), GpuSim(case, storage=storage)
+    if closure:
+        from oracle import mlp_oracle as mo
+        from periodicshiftlbm_b200.sgs import set_sgs_mlp
+
+        p = mo.random_params(2)
+        for s in (a, b):
+            for g in s.grids:
+                set_sgs_mlp(g, p, g.Info.res / s.grids[0].Info.res)
+    for _ in range(6):
+        _update(a.grids, 0, False)
+        _update(b.grids, 0, True)
+    for lev in range(3):
+        assert np.array_equal(a.populations(lev), b.populations(lev)), lev
+        assert a.grids[lev].health() == 0
+    a.close()
+    b.close()

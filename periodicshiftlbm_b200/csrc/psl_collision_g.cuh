@@ -25,8 +25,10 @@
 // are subtracted inside the last pass, so the output is g' = f' - w.
 //
 // Same physics as collide<false> (psl_collision.cuh); results agree to FP32 rounding (the
-// operation order differs).  Host-compilable (PSL_HDI) so the CPU tests can check it
-// against the oracle's collision.
+// operation order differs).  Templated on the arithmetic type: float (host-compilable,
+// PSL_HDI, so the CPU tests can check it against the oracle's collision) or a pair of FP32
+// lanes (F2, psl_pair.cuh: two cells per thread, packed FFMA2 / FADD2 / FMUL2, each lane
+// rounded as the float version rounds it).
 #pragma once
 #include <math.h>
 
@@ -34,24 +36,34 @@
 
 namespace psl {
 
+// The scalar forms of the operations the templates use; F2 overloads are in psl_pair.cuh.
+PSL_HDI float gfma(float a, float b, float c) { return fmaf(a, b, c); }
+PSL_HDI float grecip(float a) { return 1.f / a; }
+PSL_HDI float gsqrt(float a) { return sqrtf(a); }
+PSL_HDI bool all_zero(float a) { return a == 0.f; }
+PSL_HDI float sel_zero(float c, float if_zero, float other) { return c == 0.f ? if_zero : other; }
+PSL_HDI bool finite_density(float rho) { return rho > 0.f && rho < 1.0e30f; }
+
 // Ten raw moments of g: rg = sum g, j = sum c g, S_ab = sum c_a c_b g.  z-lines first
 // (3 ops per line), then y (8 per x-slot), then x (15): 66 additions.
-struct RawMomentsG {
-  float rg, jx, jy, jz, sxx, syy, szz, sxy, sxz, syz;
+template <typename T>
+struct RawMomentsGT {
+  T rg, jx, jy, jz, sxx, syy, szz, sxy, sxz, syz;
 };
 
-PSL_HDI RawMomentsG raw_moments_g(const float (&g)[27]) {
-  float z0[3][3], z1[3][3], z2[3][3];
+template <typename T>
+PSL_HDI RawMomentsGT<T> raw_moments_g(const T (&g)[27]) {
+  T z0[3][3], z1[3][3], z2[3][3];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      const float a = g[slot(i, j, 0)], b = g[slot(i, j, 1)], c = g[slot(i, j, 2)];
+      const T a = g[slot(i, j, 0)], b = g[slot(i, j, 1)], c = g[slot(i, j, 2)];
       z2[i][j] = c + a;
       z0[i][j] = z2[i][j] + b;
       z1[i][j] = c - a;
     }
-  float y00[3], y10[3], y20[3], y01[3], y11[3], y02[3];
+  T y00[3], y10[3], y20[3], y01[3], y11[3], y02[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     y20[i] = z0[i][2] + z0[i][0];
@@ -61,7 +73,7 @@ PSL_HDI RawMomentsG raw_moments_g(const float (&g)[27]) {
     y01[i] = (z1[i][2] + z1[i][0]) + z1[i][1];
     y02[i] = (z2[i][2] + z2[i][0]) + z2[i][1];
   }
-  RawMomentsG m;
+  RawMomentsGT<T> m;
   m.sxx = y00[2] + y00[0];
   m.jx = y00[2] - y00[0];
   m.rg = m.sxx + y00[1];
@@ -76,121 +88,133 @@ PSL_HDI RawMomentsG raw_moments_g(const float (&g)[27]) {
 }
 
 // Density, velocity and D (second-order central moments less rho/3 I) of a cell.
-struct CellMomentsG {
-  float rho, inv_rho, ux, uy, uz;
-  float dxx, dyy, dzz, dxy, dxz, dyz;
+template <typename T>
+struct CellMomentsGT {
+  T rho, inv_rho, ux, uy, uz;
+  T dxx, dyy, dzz, dxy, dxz, dyz;
 };
+using CellMomentsG = CellMomentsGT<float>;
 
-PSL_HDI CellMomentsG cell_moments_g(const float (&g)[27]) {
-  const RawMomentsG r = raw_moments_g(g);
-  CellMomentsG m;
-  m.rho = 1.f + r.rg;
-  m.inv_rho = 1.f / m.rho;
+template <typename T>
+PSL_HDI CellMomentsGT<T> cell_moments_g(const T (&g)[27]) {
+  const RawMomentsGT<T> r = raw_moments_g(g);
+  CellMomentsGT<T> m;
+  m.rho = T(1.f) + r.rg;
+  m.inv_rho = grecip(m.rho);
   m.ux = r.jx * m.inv_rho;
   m.uy = r.jy * m.inv_rho;
   m.uz = r.jz * m.inv_rho;
-  const float r3 = r.rg * (1.f / 3.f);
-  m.dxx = fmaf(-r.jx, m.ux, r.sxx - r3);
-  m.dyy = fmaf(-r.jy, m.uy, r.syy - r3);
-  m.dzz = fmaf(-r.jz, m.uz, r.szz - r3);
-  m.dxy = fmaf(-r.jx, m.uy, r.sxy);
-  m.dxz = fmaf(-r.jx, m.uz, r.sxz);
-  m.dyz = fmaf(-r.jy, m.uz, r.syz);
+  const T r3 = r.rg * T(1.f / 3.f);
+  m.dxx = gfma(-r.jx, m.ux, r.sxx - r3);
+  m.dyy = gfma(-r.jy, m.uy, r.syy - r3);
+  m.dzz = gfma(-r.jz, m.uz, r.szz - r3);
+  m.dxy = gfma(-r.jx, m.uy, r.sxy);
+  m.dxz = gfma(-r.jx, m.uz, r.sxz);
+  m.dyz = gfma(-r.jy, m.uz, r.syz);
   return m;
 }
 
 // Smagorinsky rate from D (include/cellFunctions.h:157-198): 1/tau without LES, else
 // 1 / (tau/2 + sqrt(tau^2 + 18 C_s |Pi_neq| / rho)/2) with |Pi_neq| = |D|.
-PSL_HDI float smagorinsky_omega_g(const CellMomentsG& m, float omega0, float tau, float tau2, float cs18) {
-  if (cs18 == 0.f) return omega0;
-  const float p2 = fmaf(m.dxx, m.dxx, fmaf(m.dyy, m.dyy, m.dzz * m.dzz)) +
-                   2.f * fmaf(m.dxy, m.dxy, fmaf(m.dxz, m.dxz, m.dyz * m.dyz));
-  const float p = sqrtf(p2);
-  return 1.f / fmaf(0.5f, tau, 0.5f * sqrtf(fmaf(cs18 * m.inv_rho, p, tau2)));
+template <typename T>
+PSL_HDI T smagorinsky_omega_g(const CellMomentsGT<T>& m, float omega0, float tau, float tau2, T cs18) {
+  if (all_zero(cs18)) return T(omega0);
+  const T p2 = gfma(m.dxx, m.dxx, gfma(m.dyy, m.dyy, m.dzz * m.dzz)) +
+               T(2.f) * gfma(m.dxy, m.dxy, gfma(m.dxz, m.dxz, m.dyz * m.dyz));
+  const T p = gsqrt(p2);
+  const T w = grecip(gfma(T(0.5f), T(tau), T(0.5f) * gsqrt(gfma(cs18 * m.inv_rho, p, T(tau2)))));
+  return sel_zero(cs18, T(omega0), w);
 }
 
 // One axis of the backward transform on pre-halved inputs (m1' = m1/2, m2' = m2/2), with
 // hu2 = u^2/2, hu = u/2, tu = 2u: (m0, m1', m2') -> (f(-1), f(0), f(+1)).
+template <typename T>
 struct BwdAxis {
-  float hu2, hu, tu;
-  PSL_HDI explicit BwdAxis(float u) : hu2(0.5f * u * u), hu(0.5f * u), tu(2.f * u) {}
+  T hu2, hu, tu;
+  PSL_HDI explicit BwdAxis(T u) : hu2(T(0.5f) * u * u), hu(T(0.5f) * u), tu(T(2.f) * u) {}
 };
 
-PSL_HDI void bwd_full(float& a, float& b, float& c, const BwdAxis& k) {
-  const float m0 = a, m1 = b, m2 = c;
-  const float h = fmaf(k.hu2, m0, fmaf(k.tu, m1, m2));
-  const float e = fmaf(k.hu, m0, m1);
+template <typename T>
+PSL_HDI void bwd_full(T& a, T& b, T& c, const BwdAxis<T>& k) {
+  const T m0 = a, m1 = b, m2 = c;
+  const T h = gfma(k.hu2, m0, gfma(k.tu, m1, m2));
+  const T e = gfma(k.hu, m0, m1);
   a = h - e;
-  b = fmaf(-2.f, h, m0);
+  b = gfma(T(-2.f), h, m0);
   c = h + e;
 }
 // m1' = 0
-PSL_HDI void bwd_even(float& a, float& b, float& c, const BwdAxis& k) {
-  const float m0 = a, m2 = c;
-  const float h = fmaf(k.hu2, m0, m2);
-  const float e = k.hu * m0;
+template <typename T>
+PSL_HDI void bwd_even(T& a, T& b, T& c, const BwdAxis<T>& k) {
+  const T m0 = a, m2 = c;
+  const T h = gfma(k.hu2, m0, m2);
+  const T e = k.hu * m0;
   a = h - e;
-  b = fmaf(-2.f, h, m0);
+  b = gfma(T(-2.f), h, m0);
   c = h + e;
 }
 // m0 = m2' = 0: f(-1) = (2u - 1) m1', f(0) = -4u m1', f(+1) = (2u + 1) m1'
-PSL_HDI void bwd_odd(float& a, float& b, float& c, float cm, float c0, float cp) {
-  const float m1 = b;
+template <typename T>
+PSL_HDI void bwd_odd(T& a, T& b, T& c, T cm, T c0, T cp) {
+  const T m1 = b;
   a = cm * m1;
   b = c0 * m1;
   c = cp * m1;
 }
 // full triple, weights subtracted: (g(-1), g(0), g(+1)) = (f(-1) - wpm, f(0) - w0, f(+1) - wpm)
-PSL_HDI void bwd_full_w(float& a, float& b, float& c, const BwdAxis& k, float wpm, float w0) {
-  const float m0 = a, m1 = b, m2 = c;
-  const float h = fmaf(k.hu2, m0, fmaf(k.tu, m1, m2)) - wpm;
-  const float e = fmaf(k.hu, m0, m1);
+template <typename T>
+PSL_HDI void bwd_full_w(T& a, T& b, T& c, const BwdAxis<T>& k, float wpm, float w0) {
+  const T m0 = a, m1 = b, m2 = c;
+  const T h = gfma(k.hu2, m0, gfma(k.tu, m1, m2)) - T(wpm);
+  const T e = gfma(k.hu, m0, m1);
   a = h - e;
-  b = fmaf(-2.f, h, m0 - (w0 + 2.f * wpm));
+  b = gfma(T(-2.f), h, m0 - T(w0 + 2.f * wpm));
   c = h + e;
 }
 
 // Post-collision g' = f' - w from rho, u and the relaxed second-order central moments
 // s** (first-order central moments zero, third-order cumulants zero; the fourth- and
 // sixth-order central moments follow as in include/applyCollision.h:178-200).
-PSL_HDI void populations_g(float (&g)[27], float rho, float inv_rho, float ux, float uy, float uz, float s200,
-                           float s020, float s002, float s011, float s101, float s110) {
+template <typename T>
+PSL_HDI void populations_g(T (&g)[27], T rho, T inv_rho, T ux, T uy, T uz, T s200, T s020, T s002, T s011, T s101,
+                           T s110) {
   // pre-scaled inputs: K[i][j][k] * 2^-(number of non-zero orders)
-  const float a200 = 0.5f * s200, a020 = 0.5f * s020, a002 = 0.5f * s002;
-  const float a011 = 0.25f * s011, a101 = 0.25f * s101, a110 = 0.25f * s110;
-  const float k211 = fmaf(a200, a011, 4.f * a101 * a110) * inv_rho;
-  const float k121 = fmaf(a020, a101, 4.f * a110 * a011) * inv_rho;
-  const float k112 = fmaf(a002, a110, 4.f * a011 * a101) * inv_rho;
-  const float k220 = fmaf(a020, a200, 8.f * a110 * a110) * inv_rho;
-  const float k022 = fmaf(a002, a020, 8.f * a011 * a011) * inv_rho;
-  const float k202 = fmaf(a200, a002, 8.f * a101 * a101) * inv_rho;
-  const float k222 =
-      (a200 * k022 + a020 * k202 + a002 * k220 + 16.f * (a011 * k211 + a101 * k121 + a110 * k112)) * inv_rho -
-      (128.f * a110 * a101 * a011 + 16.f * (a101 * a101 * a020 + a011 * a011 * a200 + a110 * a110 * a002) +
-       2.f * a200 * a020 * a002) *
+  const T a200 = T(0.5f) * s200, a020 = T(0.5f) * s020, a002 = T(0.5f) * s002;
+  const T a011 = T(0.25f) * s011, a101 = T(0.25f) * s101, a110 = T(0.25f) * s110;
+  const T k211 = gfma(a200, a011, T(4.f) * a101 * a110) * inv_rho;
+  const T k121 = gfma(a020, a101, T(4.f) * a110 * a011) * inv_rho;
+  const T k112 = gfma(a002, a110, T(4.f) * a011 * a101) * inv_rho;
+  const T k220 = gfma(a020, a200, T(8.f) * a110 * a110) * inv_rho;
+  const T k022 = gfma(a002, a020, T(8.f) * a011 * a011) * inv_rho;
+  const T k202 = gfma(a200, a002, T(8.f) * a101 * a101) * inv_rho;
+  const T k222 =
+      (a200 * k022 + a020 * k202 + a002 * k220 + T(16.f) * (a011 * k211 + a101 * k121 + a110 * k112)) * inv_rho -
+      (T(128.f) * a110 * a101 * a011 + T(16.f) * (a101 * a101 * a020 + a011 * a011 * a200 + a110 * a110 * a002) +
+       T(2.f) * a200 * a020 * a002) *
           (inv_rho * inv_rho);
 
   // G[x-slot][y-order][z-order] after the x pass
-  float G[3][3][3];
-  const BwdAxis bx(ux), by(uy), bz(uz);
-  const float xm = fmaf(2.f, ux, -1.f), x0 = -4.f * ux, xp = fmaf(2.f, ux, 1.f);
-  G[0][0][0] = rho;  G[1][0][0] = 0.f;  G[2][0][0] = a200;
+  T G[3][3][3];
+  const BwdAxis<T> bx(ux), by(uy), bz(uz);
+  const T xm = gfma(T(2.f), ux, T(-1.f)), x0 = T(-4.f) * ux, xp = gfma(T(2.f), ux, T(1.f));
+  const T zero(0.f);
+  G[0][0][0] = rho;  G[1][0][0] = zero; G[2][0][0] = a200;
   bwd_even(G[0][0][0], G[1][0][0], G[2][0][0], bx);
-  G[0][0][1] = 0.f;  G[1][0][1] = a101; G[2][0][1] = 0.f;
+  G[0][0][1] = zero; G[1][0][1] = a101; G[2][0][1] = zero;
   bwd_odd(G[0][0][1], G[1][0][1], G[2][0][1], xm, x0, xp);
-  G[0][0][2] = a002; G[1][0][2] = 0.f;  G[2][0][2] = k202;
+  G[0][0][2] = a002; G[1][0][2] = zero; G[2][0][2] = k202;
   bwd_even(G[0][0][2], G[1][0][2], G[2][0][2], bx);
-  G[0][1][0] = 0.f;  G[1][1][0] = a110; G[2][1][0] = 0.f;
+  G[0][1][0] = zero; G[1][1][0] = a110; G[2][1][0] = zero;
   bwd_odd(G[0][1][0], G[1][1][0], G[2][1][0], xm, x0, xp);
-  G[0][1][1] = a011; G[1][1][1] = 0.f;  G[2][1][1] = k211;
+  G[0][1][1] = a011; G[1][1][1] = zero; G[2][1][1] = k211;
   bwd_even(G[0][1][1], G[1][1][1], G[2][1][1], bx);
-  G[0][1][2] = 0.f;  G[1][1][2] = k112; G[2][1][2] = 0.f;
+  G[0][1][2] = zero; G[1][1][2] = k112; G[2][1][2] = zero;
   bwd_odd(G[0][1][2], G[1][1][2], G[2][1][2], xm, x0, xp);
-  G[0][2][0] = a020; G[1][2][0] = 0.f;  G[2][2][0] = k220;
+  G[0][2][0] = a020; G[1][2][0] = zero; G[2][2][0] = k220;
   bwd_even(G[0][2][0], G[1][2][0], G[2][2][0], bx);
-  G[0][2][1] = 0.f;  G[1][2][1] = k121; G[2][2][1] = 0.f;
+  G[0][2][1] = zero; G[1][2][1] = k121; G[2][2][1] = zero;
   bwd_odd(G[0][2][1], G[1][2][1], G[2][2][1], xm, x0, xp);
-  G[0][2][2] = k022; G[1][2][2] = 0.f;  G[2][2][2] = k222;
+  G[0][2][2] = k022; G[1][2][2] = zero; G[2][2][2] = k222;
   bwd_even(G[0][2][2], G[1][2][2], G[2][2][2], bx);
   // y pass
 #pragma unroll
@@ -202,7 +226,7 @@ PSL_HDI void populations_g(float (&g)[27], float rho, float inv_rho, float ux, f
   for (int a = 0; a < 3; ++a)
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
-      float m0 = G[a][b][0], m1 = G[a][b][1], m2 = G[a][b][2];
+      T m0 = G[a][b][0], m1 = G[a][b][1], m2 = G[a][b][2];
       bwd_full_w(m0, m1, m2, bz, lattice_weight(slot(a, b, 0)), lattice_weight(slot(a, b, 1)));
       g[slot(a, b, 0)] = m0;
       g[slot(a, b, 1)] = m1;
@@ -212,22 +236,23 @@ PSL_HDI void populations_g(float (&g)[27], float rho, float inv_rho, float ux, f
 
 // Relaxation at shear rate w (bulk at 1; include/applyCollision.h:119-200) from D, then
 // the backward transform: g (post-streaming deviations) -> g' (post-collision).
-PSL_HDI void relax_rebuild_g(float (&g)[27], const CellMomentsG& m, float w) {
-  const float rho = m.rho, inv_rho = m.inv_rho;
-  const float hw = 0.5f * w * inv_rho;
+template <typename T>
+PSL_HDI void relax_rebuild_g(T (&g)[27], const CellMomentsGT<T>& m, T w) {
+  const T rho = m.rho, inv_rho = m.inv_rho;
+  const T hw = T(0.5f) * w * inv_rho;
   // c200 + c020 + c002 - rho = Dxx + Dyy + Dzz;  2 c200 - c020 - c002 = 2 Dxx - Dyy - Dzz
-  const float dxu = -hw * (2.f * m.dxx - m.dyy - m.dzz) - 0.5f * inv_rho * (m.dxx + m.dyy + m.dzz);
-  const float dyv = fmaf(3.f * hw, m.dxx - m.dyy, dxu);
-  const float dzw = fmaf(3.f * hw, m.dxx - m.dzz, dxu);
-  const float om1 = 1.f - w;
-  const float ux2 = m.ux * m.ux, uy2 = m.uy * m.uy, uz2 = m.uz * m.uz;
-  const float gg = 3.f * rho * (1.f - 0.5f * w);
-  const float ea = om1 * (m.dxx - m.dyy) - gg * (ux2 * dxu - uy2 * dyv);
-  const float eb = om1 * (m.dxx - m.dzz) - gg * (ux2 * dxu - uz2 * dzw);
-  const float ec = rho - 1.5f * rho * (ux2 * dxu + uy2 * dyv + uz2 * dzw);
-  const float s200 = (1.f / 3.f) * (ea + eb + ec);
-  const float s020 = (1.f / 3.f) * (eb - 2.f * ea + ec);
-  const float s002 = (1.f / 3.f) * (ea - 2.f * eb + ec);
+  const T dxu = -hw * (T(2.f) * m.dxx - m.dyy - m.dzz) - T(0.5f) * inv_rho * (m.dxx + m.dyy + m.dzz);
+  const T dyv = gfma(T(3.f) * hw, m.dxx - m.dyy, dxu);
+  const T dzw = gfma(T(3.f) * hw, m.dxx - m.dzz, dxu);
+  const T om1 = T(1.f) - w;
+  const T ux2 = m.ux * m.ux, uy2 = m.uy * m.uy, uz2 = m.uz * m.uz;
+  const T gg = T(3.f) * rho * (T(1.f) - T(0.5f) * w);
+  const T ea = om1 * (m.dxx - m.dyy) - gg * (ux2 * dxu - uy2 * dyv);
+  const T eb = om1 * (m.dxx - m.dzz) - gg * (ux2 * dxu - uz2 * dzw);
+  const T ec = rho - T(1.5f) * rho * (ux2 * dxu + uy2 * dyv + uz2 * dzw);
+  const T s200 = T(1.f / 3.f) * (ea + eb + ec);
+  const T s020 = T(1.f / 3.f) * (eb - T(2.f) * ea + ec);
+  const T s002 = T(1.f / 3.f) * (ea - T(2.f) * eb + ec);
   populations_g(g, rho, inv_rho, m.ux, m.uy, m.uz, s200, s020, s002, om1 * m.dyz, om1 * m.dxz, om1 * m.dxy);
 }
 

@@ -12,6 +12,7 @@
 #include "psl_bc_generated.cuh"
 #include "psl_collision.cuh"
 #include "psl_collision_g.cuh"
+#include "psl_pair.cuh"
 #include "psl_hooks.cuh"
 #include "psl_lattice.cuh"
 #include "psl_storage.cuh"
@@ -140,8 +141,9 @@ __device__ __forceinline__ void apply_boundary(uint8_t m, T (&f)[27], float4 giv
 }
 
 // The collided-cell body of the 16-bit forms on the stored deviations g = f - w: the
-// boundary functions work on f (g + w, then back), the collision on g (psl_collision_g.cuh).
-// Shared by the pipelined and the batched update, so both give the same bits.
+// boundary functions work on f (g + w, then back), the collision on g (psl_collision_g.cuh)
+// in F1 arithmetic (psl_pair.cuh), so a cell gives the same bits here as in a pair of the
+// pair kernel.  Shared by the one-cell, pair and batched updates.
 __device__ __forceinline__ void collide_cell_g(int kind, uint8_t m, float (&g)[27], const float4* given,
                                                float4 given_uniform, uint32_t cell, const RelaxationT<float>& rx,
                                                float cs18, unsigned int* health, float* slot) {
@@ -152,9 +154,14 @@ __device__ __forceinline__ void collide_cell_g(int kind, uint8_t m, float (&g)[2
 #pragma unroll
     for (int q = 0; q < 27; ++q) g[q] -= lattice_weight(q);
   }
-  const CellMomentsG cm = cell_moments_g(g);
-  if (health && !(cm.rho > 0.f && cm.rho < 1.0e30f)) atomicOr(health, 1u);
-  relax_rebuild_g(g, cm, smagorinsky_omega_g(cm, rx.omega0, rx.tau, rx.tau2, cs18));
+  F1 v[27];
+#pragma unroll
+  for (int q = 0; q < 27; ++q) v[q] = F1(g[q]);
+  const CellMomentsGT<F1> cm = cell_moments_g(v);
+  if (health && !finite_density(cm.rho.v)) atomicOr(health, 1u);
+  relax_rebuild_g(v, cm, smagorinsky_omega_g(cm, rx.omega0, rx.tau, rx.tau2, F1(cs18)));
+#pragma unroll
+  for (int q = 0; q < 27; ++q) g[q] = v[q].v;
 }
 
 // Gathers / scatters of one cell through accessor A (S itself, or StoredOf<S> for the
@@ -253,14 +260,12 @@ __device__ __forceinline__ void capture_cell(const Capture<S>& cap, uint32_t cel
   for (int q = 0; q < 27; ++q) StoredOf<S>::template store<0>(dst + q, f[q]);
 }
 
-// One thread per cell.  The 16-bit forms load and store their stored values g = f - w and
-// collide on them (collide_cell_g); FP32 and FP64 run collide<false> on f, the reference's
-// operation order.
+// The update of one cell (applyLocalCellUpdate.h:21-72).  The 16-bit forms load and store
+// their stored values g = f - w and collide on them (collide_cell_g); FP32 and FP64 run
+// collide<false> on f, the reference's operation order.  `slot`: the thread's shared-memory
+// slot for the boundary functions.
 template <typename S, bool kRowIndex>
-__global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constant__ StepParams<S> p) {
-  const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
-  if (cell >= p.g.n) return;
-  const uint8_t m = p.marker[cell];
+__device__ __forceinline__ void update_one_cell(const StepParams<S>& p, uint32_t cell, uint8_t m, float* slot) {
   const int kind = marker_kind(m);
   using T = typename S::calc;
   T f[27];
@@ -280,9 +285,8 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constan
       f[q + 1] = t;
     }
   } else if constexpr (kCollidesOnG<S>) {
-    __shared__ float slot[kStepThreads][27];
     collide_cell_g(kind, m, f, p.given, p.given_uniform, cell, p.rx, p.cs ? 18.f * p.cs[cell] : p.rx.cs18, p.health,
-                   slot[threadIdx.x]);
+                   slot);
   } else {
     if (kind != kFluid) apply_boundary(m, f, p.given ? p.given[cell] : p.given_uniform);
     collide<false>(f, cell_relaxation(p.rx, p.cs, cell));
@@ -293,6 +297,77 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constan
   }
   store_for<S, kRowIndex>(p, cell, f);
   capture_cell(p.cap, cell, f);
+}
+
+// One thread per cell.
+template <typename S, bool kRowIndex>
+__global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constant__ StepParams<S> p) {
+  const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
+  if (cell >= p.g.n) return;
+  if constexpr (kCollidesOnG<S>) {
+    __shared__ float slot[kStepThreads][27];
+    update_one_cell<S, kRowIndex>(p, cell, p.marker[cell], slot[threadIdx.x]);
+  } else {
+    update_one_cell<S, kRowIndex>(p, cell, p.marker[cell], nullptr);
+  }
+}
+
+// Two adjacent cells per thread for the 16-bit forms (cells a = 2k and a + 1, N even): a
+// pair of plain fluid cells collides as one F2 value (psl_pair.cuh), every +, - and * of
+// the g-form collision one packed instruction for both cells; any other pair takes the
+// one-cell body per cell.  Population q of cell a + 1 is the element after cell a's, except
+// where the row's wrap point falls between them.
+template <typename S, int Q = 0>
+__device__ __forceinline__ void load_pair(const RowIndex<S>& r, uint32_t a, F2 (&g)[27]) {
+  if constexpr (Q < 27) {
+    uint32_t i = a + r.off[Q];
+    if (a >= r.lim[Q]) i -= r.n;
+    const uint32_t i1 = a + 1 == r.lim[Q] ? i + 1 - r.n : i + 1;
+    g[Q] = F2(StoredOf<S>::template load_once<Q>(r.base + i), StoredOf<S>::template load_once<Q>(r.base + i1));
+    load_pair<S, Q + 1>(r, a, g);
+  }
+}
+template <typename S, int Q = 0>
+__device__ __forceinline__ void store_pair(const RowIndex<S>& r, uint32_t a, const F2 (&g)[27]) {
+  if constexpr (Q < 27) {
+    uint32_t i = a + r.off[Q];
+    if (a >= r.lim[Q]) i -= r.n;
+    const uint32_t i1 = a + 1 == r.lim[Q] ? i + 1 - r.n : i + 1;
+    StoredOf<S>::template store_once<Q>(r.base + i, g[Q].v.x);
+    StoredOf<S>::template store_once<Q>(r.base + i1, g[Q].v.y);
+    store_pair<S, Q + 1>(r, a, g);
+  }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kStepThreads) step_pair_kernel(const __grid_constant__ StepParams<S> p) {
+  static_assert(kCollidesOnG<S>, "the pair kernel serves the 16-bit forms");
+  __shared__ float slot[kStepThreads][27];
+  const uint32_t a = 2u * (blockIdx.x * kStepThreads + threadIdx.x);
+  if (a >= p.ri.n) return;
+  const uint8_t mA = p.marker[a], mB = p.marker[a + 1];
+  if (marker_kind(mA) != kFluid || marker_kind(mB) != kFluid) {
+    update_one_cell<S, true>(p, a, mA, slot[threadIdx.x]);
+    update_one_cell<S, true>(p, a + 1, mB, slot[threadIdx.x]);
+    return;
+  }
+  F2 g[27];
+  load_pair<S>(p.ri, a, g);
+  const CellMomentsGT<F2> cm = cell_moments_g(g);
+  if (p.health && !(finite_density(cm.rho.v.x) && finite_density(cm.rho.v.y))) atomicOr(p.health, 1u);
+  const F2 cs18 = p.cs ? F2(18.f * p.cs[a], 18.f * p.cs[a + 1]) : F2(p.rx.cs18);
+  relax_rebuild_g(g, cm, smagorinsky_omega_g(cm, p.rx.omega0, p.rx.tau, p.rx.tau2, cs18));
+  store_pair<S>(p.ri, a, g);
+  if (p.cap.buf) {
+    float fa[27], fb[27];
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+      fa[q] = g[q].v.x;
+      fb[q] = g[q].v.y;
+    }
+    capture_cell(p.cap, a, fa);
+    capture_cell(p.cap, a + 1, fb);
+  }
 }
 
 // ------------------------------------------------------------------------------------------

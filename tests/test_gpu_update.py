@@ -2,10 +2,12 @@
 coarse/fine restriction's capture.
 
 * Grids and shifts that exercise the shifted addressing -- one 128-cell block, several
-  blocks with a partial last one, shifts whose wrap point falls inside a block, arbitrary
-  shifts -- for every storage form, with and without a per-cell C_s field, with skipped
-  and solid cells among the fluid ones: every cell against the oracle's collision (FP64),
-  skipped cells unchanged and solid cells bounced back bit for bit.
+  blocks with a partial last one, shifts whose wrap point falls inside a block or between
+  the two cells of a pair (the 16-bit forms' pair kernel), an odd cell count (one cell per
+  thread), arbitrary shifts -- for every storage form, with and without a per-cell C_s
+  field, with skipped and solid cells among the fluid ones: every cell against the
+  oracle's collision (FP64), skipped cells unchanged and solid cells bounced back bit for
+  bit.
 * A refined LES sphere run whose coarse grid has a per-cell C_s (a sponge ahead of the
   outlet, getSmagorinskyConstant per cell) against the reference's own update run live.
 * The x-face ring cells restricted from the fine update's capture against the restriction
@@ -38,7 +40,7 @@ def _start(orc, n, rng):
 
 
 @pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
-@pytest.mark.parametrize("dims", [(12, 4, 2), (20, 3, 8), (16, 8, 8), (40, 12, 12)])
+@pytest.mark.parametrize("dims", [(12, 4, 2), (20, 3, 8), (16, 8, 8), (40, 12, 12), (7, 5, 3)])
 @pytest.mark.parametrize("field", [False, True])
 def test_update_matches_oracle_for_any_shift(orc, storage, dims, field):
     nx, ny, nz = dims

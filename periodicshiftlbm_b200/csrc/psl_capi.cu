@@ -501,12 +501,6 @@ static cudaError_t launch_step(psl_grid* g) {
     p.ri.lim[q] = g->n - g->shift[q];
   }
   const bool row_index = 27 * g->stride + g->n < (1ull << 32);
-  if constexpr (kCollidesOnG<S>) {
-    if (row_index && g->n % 2 == 0) {  // two cells per thread
-      step_pair_kernel<S><<<blocks_for(g->n / 2, kStepThreads), kStepThreads, 0, g->stream>>>(p);
-      return cudaGetLastError();
-    }
-  }
   if (row_index)
     step_kernel<S, true><<<blocks_for(g->n, kStepThreads), kStepThreads, 0, g->stream>>>(p);
   else

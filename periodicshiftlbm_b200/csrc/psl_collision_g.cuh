@@ -25,10 +25,8 @@
 // are subtracted inside the last pass, so the output is g' = f' - w.
 //
 // Same physics as collide<false> (psl_collision.cuh); results agree to FP32 rounding (the
-// operation order differs).  Templated on the arithmetic type: float (host-compilable,
-// PSL_HDI, so the CPU tests can check it against the oracle's collision) or a pair of FP32
-// lanes (F2, psl_pair.cuh: two cells per thread, packed FFMA2 / FADD2 / FMUL2, each lane
-// rounded as the float version rounds it).
+// operation order differs).  Templated on the arithmetic type (float everywhere today;
+// host-compilable, PSL_HDI, so the CPU tests can check it against the oracle's collision).
 #pragma once
 #include <math.h>
 
@@ -36,7 +34,7 @@
 
 namespace psl {
 
-// The scalar forms of the operations the templates use; F2 overloads are in psl_pair.cuh.
+// The scalar forms of the operations the templates use.
 PSL_HDI float gfma(float a, float b, float c) { return fmaf(a, b, c); }
 PSL_HDI float grecip(float a) { return 1.f / a; }
 PSL_HDI float gsqrt(float a) { return sqrtf(a); }

@@ -12,7 +12,6 @@
 #include "psl_bc_generated.cuh"
 #include "psl_collision.cuh"
 #include "psl_collision_g.cuh"
-#include "psl_pair.cuh"
 #include "psl_hooks.cuh"
 #include "psl_lattice.cuh"
 #include "psl_storage.cuh"
@@ -141,9 +140,8 @@ __device__ __forceinline__ void apply_boundary(uint8_t m, T (&f)[27], float4 giv
 }
 
 // The collided-cell body of the 16-bit forms on the stored deviations g = f - w: the
-// boundary functions work on f (g + w, then back), the collision on g (psl_collision_g.cuh)
-// in F1 arithmetic (psl_pair.cuh), so a cell gives the same bits here as in a pair of the
-// pair kernel.  Shared by the one-cell, pair and batched updates.
+// boundary functions work on f (g + w, then back), the collision on g (psl_collision_g.cuh).
+// Shared by the one-cell and the batched update, so both give the same bits.
 __device__ __forceinline__ void collide_cell_g(int kind, uint8_t m, float (&g)[27], const float4* given,
                                                float4 given_uniform, uint32_t cell, const RelaxationT<float>& rx,
                                                float cs18, unsigned int* health, float* slot) {
@@ -154,14 +152,9 @@ __device__ __forceinline__ void collide_cell_g(int kind, uint8_t m, float (&g)[2
 #pragma unroll
     for (int q = 0; q < 27; ++q) g[q] -= lattice_weight(q);
   }
-  F1 v[27];
-#pragma unroll
-  for (int q = 0; q < 27; ++q) v[q] = F1(g[q]);
-  const CellMomentsGT<F1> cm = cell_moments_g(v);
-  if (health && !finite_density(cm.rho.v)) atomicOr(health, 1u);
-  relax_rebuild_g(v, cm, smagorinsky_omega_g(cm, rx.omega0, rx.tau, rx.tau2, F1(cs18)));
-#pragma unroll
-  for (int q = 0; q < 27; ++q) g[q] = v[q].v;
+  const CellMomentsG cm = cell_moments_g(g);
+  if (health && !finite_density(cm.rho)) atomicOr(health, 1u);
+  relax_rebuild_g(g, cm, smagorinsky_omega_g(cm, rx.omega0, rx.tau, rx.tau2, cs18));
 }
 
 // Gathers / scatters of one cell through accessor A (S itself, or StoredOf<S> for the
@@ -309,64 +302,6 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constan
     update_one_cell<S, kRowIndex>(p, cell, p.marker[cell], slot[threadIdx.x]);
   } else {
     update_one_cell<S, kRowIndex>(p, cell, p.marker[cell], nullptr);
-  }
-}
-
-// Two adjacent cells per thread for the 16-bit forms (cells a = 2k and a + 1, N even): a
-// pair of plain fluid cells collides as one F2 value (psl_pair.cuh), every +, - and * of
-// the g-form collision one packed instruction for both cells; any other pair takes the
-// one-cell body per cell.  Population q of cell a + 1 is the element after cell a's, except
-// where the row's wrap point falls between them.
-template <typename S, int Q = 0>
-__device__ __forceinline__ void load_pair(const RowIndex<S>& r, uint32_t a, F2 (&g)[27]) {
-  if constexpr (Q < 27) {
-    uint32_t i = a + r.off[Q];
-    if (a >= r.lim[Q]) i -= r.n;
-    const uint32_t i1 = a + 1 == r.lim[Q] ? i + 1 - r.n : i + 1;
-    g[Q] = F2(StoredOf<S>::template load_once<Q>(r.base + i), StoredOf<S>::template load_once<Q>(r.base + i1));
-    load_pair<S, Q + 1>(r, a, g);
-  }
-}
-template <typename S, int Q = 0>
-__device__ __forceinline__ void store_pair(const RowIndex<S>& r, uint32_t a, const F2 (&g)[27]) {
-  if constexpr (Q < 27) {
-    uint32_t i = a + r.off[Q];
-    if (a >= r.lim[Q]) i -= r.n;
-    const uint32_t i1 = a + 1 == r.lim[Q] ? i + 1 - r.n : i + 1;
-    StoredOf<S>::template store_once<Q>(r.base + i, g[Q].v.x);
-    StoredOf<S>::template store_once<Q>(r.base + i1, g[Q].v.y);
-    store_pair<S, Q + 1>(r, a, g);
-  }
-}
-
-template <typename S>
-__global__ void __launch_bounds__(kStepThreads) step_pair_kernel(const __grid_constant__ StepParams<S> p) {
-  static_assert(kCollidesOnG<S>, "the pair kernel serves the 16-bit forms");
-  __shared__ float slot[kStepThreads][27];
-  const uint32_t a = 2u * (blockIdx.x * kStepThreads + threadIdx.x);
-  if (a >= p.ri.n) return;
-  const uint8_t mA = p.marker[a], mB = p.marker[a + 1];
-  if (marker_kind(mA) != kFluid || marker_kind(mB) != kFluid) {
-    update_one_cell<S, true>(p, a, mA, slot[threadIdx.x]);
-    update_one_cell<S, true>(p, a + 1, mB, slot[threadIdx.x]);
-    return;
-  }
-  F2 g[27];
-  load_pair<S>(p.ri, a, g);
-  const CellMomentsGT<F2> cm = cell_moments_g(g);
-  if (p.health && !(finite_density(cm.rho.v.x) && finite_density(cm.rho.v.y))) atomicOr(p.health, 1u);
-  const F2 cs18 = p.cs ? F2(18.f * p.cs[a], 18.f * p.cs[a + 1]) : F2(p.rx.cs18);
-  relax_rebuild_g(g, cm, smagorinsky_omega_g(cm, p.rx.omega0, p.rx.tau, p.rx.tau2, cs18));
-  store_pair<S>(p.ri, a, g);
-  if (p.cap.buf) {
-    float fa[27], fb[27];
-#pragma unroll
-    for (int q = 0; q < 27; ++q) {
-      fa[q] = g[q].v.x;
-      fb[q] = g[q].v.y;
-    }
-    capture_cell(p.cap, a, fa);
-    capture_cell(p.cap, a + 1, fb);
   }
 }
 
@@ -810,6 +745,7 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
     const uint32_t faceJ = 2u * a * (c - 2);
     PSL_FOR_EACH_ITEM(t, p.n_ring) {
       int ri, rj, rk;
+      int xface = -1;  // x-face ring cells read their children from the capture
       if (t < faceK) {
         const uint32_t layer = t / (a * b), r = t % (a * b);
         rk = layer ? c - 1 : 0;
@@ -825,12 +761,10 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
         ri = layer ? a - 1 : 0;
         rj = 1 + r % (b - 2);
         rk = 1 + r / (b - 2);
-        if (p.xcap) {
-          restrict_cell(rc, rf, p, p.iS + 1 + ri, p.jS + 1 + rj, p.kS + 1 + rk, (int)layer);
-          continue;
-        }
+        if (p.xcap) xface = (int)layer;
       }
-      restrict_cell(rc, rf, p, p.iS + 1 + ri, p.jS + 1 + rj, p.kS + 1 + rk);
+      // one call site: the rescale is inlined once
+      restrict_cell(rc, rf, p, p.iS + 1 + ri, p.jS + 1 + rj, p.kS + 1 + rk, xface);
     }
   }
   grid_barrier(p.barrier, p.nblocks, p.error);

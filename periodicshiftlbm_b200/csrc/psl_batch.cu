@@ -323,7 +323,6 @@ int psl_batch_run(psl_batch* b, int steps) {
                   PSL_ERR_INVALID, "psl_batch_run: a member grid was streamed outside the batch");
   int rc = wait_for_members(b);
   if (rc) return rc;
-  for (psl_grid* g : b->grids) psl_detail_touch(g);
   if (!b->graph) {
     rc = capture_graph(b);
     if (rc) return rc;

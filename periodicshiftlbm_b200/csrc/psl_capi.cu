@@ -181,7 +181,6 @@ int psl_grid_destroy(psl_grid* g) {
   if (g->T) cudaFree(g->T);
   if (g->givenT) cudaFree(g->givenT);
   if (g->cs_field) cudaFree(g->cs_field);
-  if (g->xcap) cudaFree(g->xcap);
   delete g;
   return PSL_OK;
 }
@@ -412,7 +411,6 @@ int psl_set_smagorinsky_field(psl_grid* g, const float* host_cs) {
 template <typename Case>
 static int fill_eq(psl_grid* g, const Case& c) {
   DeviceGuard dg(g->device);
-  psl_detail_touch(g);
   const unsigned int nb = blocks_for(g->n, 256);
   with_storage(g->storage, [&](auto s) {
     using S = decltype(s);
@@ -437,7 +435,6 @@ int psl_fill_equilibrium_uniform(psl_grid* g, float rho, float ux, float uy, flo
 int psl_fill_equilibrium_field(psl_grid* g, const float* rho_u) {
   PSL_CHECK(g && rho_u, PSL_ERR_INVALID, "psl_fill_equilibrium_field: null argument");
   DeviceGuard dg(g->device);
-  psl_detail_touch(g);
   float* tmp = nullptr;
   PSL_CUDA(cudaMalloc(&tmp, (size_t)g->n * 4 * sizeof(float)));
   cudaError_t e = cudaMemcpyAsync(tmp, rho_u, (size_t)g->n * 4 * sizeof(float), cudaMemcpyHostToDevice, g->stream);
@@ -457,7 +454,6 @@ int psl_fill_equilibrium_field(psl_grid* g, const float* rho_u) {
 
 int psl_apply_streaming(psl_grid* g) {
   PSL_CHECK(g, PSL_ERR_INVALID, "psl_apply_streaming: null grid");
-  psl_detail_touch(g);
   const long long nx = g->info.cell_count_x, ny = g->info.cell_count_y, n = g->n;
   for (int q = 0; q < 27; ++q) {
     long long s = (long long)g->shift[q];
@@ -493,7 +489,6 @@ static cudaError_t launch_step(psl_grid* g) {
   p.cs = g->cs_field;
   p.rx = relaxation<typename S::calc>(g);
   p.health = g->health;
-  psl_detail_fill_capture(g, p.cap);
   p.ri.base = static_cast<typename S::type*>(g->f);
   p.ri.n = g->n;
   for (int q = 0; q < 27; ++q) {
@@ -511,7 +506,6 @@ static cudaError_t launch_step(psl_grid* g) {
 int psl_apply_local_cell_update(psl_grid* g) {
   PSL_CHECK(g, PSL_ERR_INVALID, "psl_apply_local_cell_update: null grid");
   DeviceGuard dg(g->device);
-  psl_detail_touch(g);
   const bool custom = g->custom_markers || g->body.x != 0.f || g->body.y != 0.f || g->body.z != 0.f;
   if (g->T) {
     PSL_CHECK(!custom && !g->mlp, PSL_ERR_INVALID,
@@ -529,7 +523,6 @@ int psl_apply_local_cell_update(psl_grid* g) {
         sp.base.given = g->given;
         sp.base.given_uniform = g->given_uniform;
         sp.base.cs = g->cs_field;
-        sp.base.cap = Capture<S>{};
         sp.base.rx = relaxation<float>(g);
         sp.base.health = g->health;
         sp.T.base = g->T;
@@ -565,7 +558,6 @@ int psl_apply_local_cell_update(psl_grid* g) {
         cp.base.given = g->given;
         cp.base.given_uniform = g->given_uniform;
         cp.base.cs = g->cs_field;
-        cp.base.cap = Capture<S>{};
         cp.base.rx = relaxation<float>(g);
         cp.base.health = g->health;
         cp.body = g->body;
@@ -593,7 +585,6 @@ static void launch_periodic(psl_grid* g, int axis) {
 static int periodic(psl_grid* g, int axis) {
   PSL_CHECK(g, PSL_ERR_INVALID, "psl_apply_bc_periodic: null grid");
   DeviceGuard dg(g->device);
-  psl_detail_touch(g);
   with_storage(g->storage, [&](auto s) {
     launch_periodic<decltype(s)>(g, axis);
     return 0;
@@ -605,7 +596,7 @@ int psl_apply_bc_periodic_x(psl_grid* g) { return periodic(g, 0); }
 int psl_apply_bc_periodic_y(psl_grid* g) { return periodic(g, 1); }
 
 template <typename S>
-static int launch_coarse_fine(psl_grid* c, psl_grid* f, bool use_capture) {
+static int launch_coarse_fine(psl_grid* c, psl_grid* f) {
   const psl_info& C = c->info;
   const psl_info& F = f->info;
   const int a = C.i_subgrid_end - C.i_subgrid_start, b = C.j_subgrid_end - C.j_subgrid_start,
@@ -634,7 +625,6 @@ static int launch_coarse_fine(psl_grid* c, psl_grid* f, bool use_capture) {
   p.n_shell = (uint32_t)((long long)p.fnx * p.fny * p.fnz - (long long)(p.fnx - 4) * (p.fny - 4) * (p.fnz - 4));
   p.barrier = c->health + 1;
   p.error = c->health;
-  p.xcap = use_capture ? static_cast<const typename S::type*>(f->xcap) : nullptr;
   int sms = 0, per_sm = 0;
   PSL_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
   PSL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_fine_kernel<S>, kCoarseFineThreads, 0));
@@ -689,7 +679,6 @@ int psl_fill_coarse_grid_from_fine(psl_grid* c, psl_grid* f) {
   PSL_CHECK(27ull * c->stride + c->n < (1ull << 32) && 27ull * f->stride + f->n < (1ull << 32), PSL_ERR_INVALID,
             "fill coarse: grid too large for 32-bit row offsets");
   DeviceGuard dg(c->device);
-  psl_detail_touch(c);
   return with_storage(c->storage, [&](auto s) { return launch_fill_coarse<decltype(s)>(c, f); });
 }
 
@@ -708,21 +697,7 @@ int psl_apply_coarse_fine_grid_communication(psl_grid* c, psl_grid* f) {
   PSL_CHECK(27ull * c->stride + c->n < (1ull << 32) && 27ull * f->stride + f->n < (1ull << 32), PSL_ERR_INVALID,
             "coarse/fine: grid too large for 32-bit row offsets");
   DeviceGuard dg(c->device);
-  // The fine grid's x-face ring children come from its update's capture when its last
-  // population change was a capturing update; the first transfer sets the capture up.
-  const bool use_capture = f->xcap && f->xcap_version == f->state_version;
-  if (!f->xcap && f->storage != kStoreF64 && F.cell_count_x >= 8) {
-    const size_t bytes = 2ull * F.cell_count_y * F.cell_count_z * 2 * 27 * storage_bytes(f->storage);
-    if (cudaMalloc(&f->xcap, bytes) != cudaSuccess) {
-      f->xcap = nullptr;  // no capture: the transfer reads the fine grid itself
-      cudaGetLastError();
-    }
-    f->xcap_i0 = 2;                     // children of ring cell iS + 1
-    f->xcap_i1 = F.cell_count_x - 4;    // children of ring cell iE - 2
-  }
-  psl_detail_touch(c);
-  psl_detail_touch(f);
-  return with_storage(c->storage, [&](auto s) { return launch_coarse_fine<decltype(s)>(c, f, use_capture); });
+  return with_storage(c->storage, [&](auto s) { return launch_coarse_fine<decltype(s)>(c, f); });
 }
 
 int psl_update_grid(psl_grid** grids, int levels, int level) {
@@ -799,7 +774,6 @@ static int gather(psl_grid* g, float* host) {
 
 template <typename S>
 static int scatter(psl_grid* g, const float* host) {
-  psl_detail_touch(g);
   float* tmp = nullptr;
   PSL_CUDA(cudaMalloc(&tmp, (size_t)g->n * sizeof(float)));
   cudaError_t e = cudaSuccess;
@@ -860,7 +834,6 @@ int psl_set_shifts(psl_grid* g, const int* s) {
   PSL_CHECK(g && s, PSL_ERR_INVALID, "psl_set_shifts: null argument");
   for (int q = 0; q < 27; ++q)
     PSL_CHECK(s[q] >= 0 && (uint32_t)s[q] < g->n, PSL_ERR_INVALID, "psl_set_shifts: shift outside [0, N)");
-  psl_detail_touch(g);
   for (int q = 0; q < 27; ++q) g->shift[q] = (uint32_t)s[q];
   return PSL_OK;
 }

@@ -40,13 +40,6 @@ struct psl_grid {
   float4 given_uniform = make_float4(1.f, 0.f, 0.f, 0.f);
   float cs = 0.f;
   float* cs_field = nullptr;        // per-cell Smagorinsky constants (getSmagorinskyConstant), or null
-  // Capture of the x-face ring cells' children for the coarse/fine restriction (a fine
-  // grid's update writes it, Capture in psl_kernels.cuh): allocated by the first transfer,
-  // used while the fine grid's last population change was a capturing update.
-  void* xcap = nullptr;
-  int xcap_i0 = 0, xcap_i1 = 0;     // first fine column of each captured pair
-  unsigned long long state_version = 0;  // bumped by every call that changes the populations
-  unsigned long long xcap_version = 0;   // state_version the capture belongs to
   uint32_t shift[27] = {};
   cudaStream_t stream = 0;
   unsigned int* health = nullptr;   // [0] health bits, [1] barrier counter
@@ -62,27 +55,6 @@ struct psl_grid {
   float mlp_width = 1.f;            // filter width fed to the closure
   float mlp_scalars[24] = {};       // its normalisation, b3, output scale (psl::MlpScalars)
 };
-
-// Every call that changes a grid's populations or shifts calls this first.
-inline void psl_detail_touch(psl_grid* g) { ++g->state_version; }
-
-// The capture a fine grid's update writes for the coarse/fine restriction (Capture<S>,
-// psl_kernels.cuh; buf null when the grid has none); marks the grid's current state as
-// captured.  The row of a cell is cell / Nx by multiply-shift: s = 31 + ceil(log2 Nx),
-// m = floor(2^s / Nx) + 1, exact for every cell < 2^31.
-template <typename C>
-inline void psl_detail_fill_capture(psl_grid* g, C& cap) {
-  cap.buf = static_cast<decltype(cap.buf)>(g->xcap);
-  cap.nx = (uint32_t)g->info.cell_count_x;
-  cap.rows = (uint32_t)g->info.cell_count_y * (uint32_t)g->info.cell_count_z;
-  cap.i0 = (uint32_t)g->xcap_i0;
-  cap.i1 = (uint32_t)g->xcap_i1;
-  uint32_t log2_nx = 0;
-  while ((1ull << log2_nx) < cap.nx) ++log2_nx;
-  cap.div_s = 31 + log2_nx;
-  cap.div_m = ((1ull << cap.div_s) / cap.nx) + 1;
-  if (g->xcap) g->xcap_version = g->state_version;
-}
 
 // Launches the update kernel with the learned closure (psl_learned.cu); status as psl_*.
 __attribute__((visibility("hidden"))) int psl_detail_launch_learned(psl_grid* g);

@@ -50,34 +50,6 @@ struct RowIndex {
   uint32_t n;
 };
 
-// The coarse/fine restriction's capture (a fine grid's update writes it): after its
-// update, each cell of fine columns i0, i0 + 1 (face 0) and i1, i1 + 1 (face 1) writes
-// its 27 stored values to buf[((face * rows + row) * 2 + column) * 27 + q], row = k Ny + j.
-// The row of a cell is cell / Nx by an exact multiply-shift: (cell * m) >> s with
-// s = 31 + ceil(log2 Nx), m = floor(2^s / Nx) + 1 (exact for every cell < 2^31).
-template <typename S>
-struct Capture {
-  typename S::type* buf;   // null: no capture
-  uint32_t nx, rows, i0, i1;
-  unsigned long long div_m;
-  uint32_t div_s;
-  // the slot of `cell`'s values, or null when its column is not captured
-  __device__ __forceinline__ typename S::type* slot(uint32_t cell) const {
-    const uint32_t row = (uint32_t)(((unsigned long long)cell * div_m) >> div_s);
-    const uint32_t i = cell - row * nx;
-    uint32_t face, col;
-    if (i - i0 < 2u) {
-      face = 0;
-      col = i - i0;
-    } else if (i - i1 < 2u) {
-      face = 1;
-      col = i - i1;
-    } else {
-      return nullptr;
-    }
-    return buf + ((size_t)(face * rows + row) * 2 + col) * 27;
-  }
-};
 
 template <typename S>
 struct StepParams {
@@ -89,7 +61,6 @@ struct StepParams {
   const float* cs;       // per-cell Smagorinsky constant (getSmagorinskyConstant), or null: rx.cs18
   RelaxationT<typename S::calc> rx;
   unsigned int* health;  // bit 0 set when a collided cell's density is not finite/positive
-  Capture<S> cap;        // the fine grid's capture for the coarse/fine restriction (cap.buf null: none)
 };
 
 // The relaxation parameters of one cell: the grid's, with the cell's own Smagorinsky
@@ -243,16 +214,6 @@ __device__ __forceinline__ void store_for(const StepParams<S>& p, uint32_t cell,
   if constexpr (kRowIndex) store_cell_as<A>(p.ri, cell, f);
   else store_cell_as<A>(p.g, cell, f);
 }
-// The cell's stored values into the capture, when its column is captured.
-template <typename S>
-__device__ __forceinline__ void capture_cell(const Capture<S>& cap, uint32_t cell, const typename S::calc (&f)[27]) {
-  if (!cap.buf) return;
-  typename S::type* dst = cap.slot(cell);
-  if (!dst) return;
-#pragma unroll
-  for (int q = 0; q < 27; ++q) StoredOf<S>::template store<0>(dst + q, f[q]);
-}
-
 // The update of one cell (applyLocalCellUpdate.h:21-72).  The 16-bit forms load and store
 // their stored values g = f - w and collide on them (collide_cell_g); FP32 and FP64 run
 // collide<false> on f, the reference's operation order.  `slot`: the thread's shared-memory
@@ -262,13 +223,7 @@ __device__ __forceinline__ void update_one_cell(const StepParams<S>& p, uint32_t
   const int kind = marker_kind(m);
   using T = typename S::calc;
   T f[27];
-  if (kind == kSkip) {  // not updated; a captured column still records its values
-    if (p.cap.buf && p.cap.slot(cell)) {
-      load_for<S, kRowIndex>(p, cell, f);
-      capture_cell(p.cap, cell, f);
-    }
-    return;
-  }
+  if (kind == kSkip) return;
   load_for<S, kRowIndex>(p, cell, f);
   if (kind == kSolid) {  // bounce-back: g and f swap alike (w_q = w_opposite(q))
 #pragma unroll
@@ -289,7 +244,6 @@ __device__ __forceinline__ void update_one_cell(const StepParams<S>& p, uint32_t
     }
   }
   store_for<S, kRowIndex>(p, cell, f);
-  capture_cell(p.cap, cell, f);
 }
 
 // One thread per cell.
@@ -617,9 +571,6 @@ struct CoarseFineParams {
   unsigned int* barrier;    // zeroed before launch
   unsigned int* error;      // bit 1: barrier gave up
   unsigned int nblocks;
-  // The fine update's capture of the x-face ring cells' children (Capture, above):
-  // [2 faces][fine rows][2 columns][27] stored values, or null (read from the fine grid).
-  const typename S::type* xcap;
 };
 
 // direction sets streaming inward across each face (gridRefinementFunctions.h:441-446):
@@ -672,12 +623,10 @@ constexpr int kCoarseFineThreads = 128;
 
 // Coarse cell (i, j, k) of the refined block from its 8 fine children: their populations
 // added in the child order (k, j, i outer to inner), averaged, rescaled fine -> coarse
-// (writeToCoarseGridInterface, gridRefinementFunctions.h:283-336).  With `xface` >= 0 the
-// children come from the fine update's capture of that x face (the same stored values in
-// the same order, so the same sums): fine columns 0 and 1 of the face's captured pair.
+// (writeToCoarseGridInterface, gridRefinementFunctions.h:283-336).
 template <typename S>
 __device__ __forceinline__ void restrict_cell(const RowIndex<S>& rc, const RowIndex<S>& rf, const CoarseFineParams<S>& p,
-                                              int i, int j, int k, int xface = -1) {
+                                              int i, int j, int k) {
   using T = typename S::calc;
   const int fi = (i - p.iS) * 2, fj = (j - p.jS) * 2, fk = (k - p.kS) * 2;
   T f[27];
@@ -689,16 +638,9 @@ __device__ __forceinline__ void restrict_cell(const RowIndex<S>& rc, const RowIn
     for (int dj = 0; dj <= 1; ++dj)
 #pragma unroll
       for (int di = 0; di <= 1; ++di) {
-        if (xface >= 0) {
-          const typename S::type* src =
-              p.xcap + (((size_t)xface * p.fny * p.fnz + (uint32_t)(fk + dk) * p.fny + (fj + dj)) * 2 + di) * 27;
+        const uint32_t fc = ((uint32_t)(fk + dk) * p.fny + (fj + dj)) * p.fnx + (fi + di);
 #pragma unroll
-          for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], S::load_q(src + q, q));
-        } else {
-          const uint32_t fc = ((uint32_t)(fk + dk) * p.fny + (fj + dj)) * p.fnx + (fi + di);
-#pragma unroll
-          for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], load_pop(rf, q, fc));
-        }
+        for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], load_pop(rf, q, fc));
       }
 #pragma unroll
   for (int q = 0; q < 27; ++q) f[q] = f[q] * T(0.125);
@@ -745,7 +687,6 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
     const uint32_t faceJ = 2u * a * (c - 2);
     PSL_FOR_EACH_ITEM(t, p.n_ring) {
       int ri, rj, rk;
-      int xface = -1;  // x-face ring cells read their children from the capture
       if (t < faceK) {
         const uint32_t layer = t / (a * b), r = t % (a * b);
         rk = layer ? c - 1 : 0;
@@ -761,10 +702,8 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
         ri = layer ? a - 1 : 0;
         rj = 1 + r % (b - 2);
         rk = 1 + r / (b - 2);
-        if (p.xcap) xface = (int)layer;
       }
-      // one call site: the rescale is inlined once
-      restrict_cell(rc, rf, p, p.iS + 1 + ri, p.jS + 1 + rj, p.kS + 1 + rk, xface);
+      restrict_cell(rc, rf, p, p.iS + 1 + ri, p.jS + 1 + rj, p.kS + 1 + rk);
     }
   }
   grid_barrier(p.barrier, p.nblocks, p.error);

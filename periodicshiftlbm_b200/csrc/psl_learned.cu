@@ -124,7 +124,6 @@ int launch(psl_grid* g) {
   p.width = g->mlp_width;
   p.n = g->n;
   p.health = g->health;
-  psl_detail_fill_capture(g, p.cap);
   step_learned_warp_kernel<S><<<(g->n + kStepThreads - 1) / kStepThreads, kStepThreads, 0, g->stream>>>(p);
   MLP_CUDA(cudaGetLastError());
   return PSL_OK;

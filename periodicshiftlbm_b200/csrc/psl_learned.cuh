@@ -31,7 +31,6 @@ struct LearnedParams {
   float width;              // filter width fed to the closure (cell size / coarsest cell size)
   uint32_t n;
   unsigned int* health;
-  Capture<S> cap;            // the fine grid's capture for the coarse/fine restriction
 };
 
 // The closure's features from D = C - rho/3 I (the g-form moments): the same quantities
@@ -69,14 +68,7 @@ __global__ void __launch_bounds__(kStepThreads, 6) step_learned_warp_kernel(cons
   using A = StoredOf<S>;
   float x[kMlpIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   float f[27];
-  if (kind == kSkip) {
-    if (cell < p.n && p.cap.buf && p.cap.slot(cell)) {  // a captured column records its values
-      load_cell_as<A>(p.ri, cell, f);
-      capture_cell(p.cap, cell, f);
-    }
-  } else {
-    load_cell_as<A>(p.ri, cell, f);
-  }
+  if (kind != kSkip) load_cell_as<A>(p.ri, cell, f);
   if (kind == kSolid) {  // bounce-back: done before the closure, nothing to keep
 #pragma unroll
     for (int q = 1; q < 27; q += 2) {
@@ -85,7 +77,6 @@ __global__ void __launch_bounds__(kStepThreads, 6) step_learned_warp_kernel(cons
       f[q + 1] = t;
     }
     store_cell_as<A>(p.ri, cell, f);
-    capture_cell(p.cap, cell, f);
   }
   const bool collides = kind != kSkip && kind != kSolid;
   if constexpr (kCollidesOnG<S>) {
@@ -107,7 +98,6 @@ __global__ void __launch_bounds__(kStepThreads, 6) step_learned_warp_kernel(cons
     if (collides) {
       relax_rebuild_g(f, cm, 1.f / (3.f * (p.nu + nu_t) + 0.5f));
       store_cell_as<A>(p.ri, cell, f);
-      capture_cell(p.cap, cell, f);
     }
   } else {
     float K[3][3][3];
@@ -126,7 +116,6 @@ __global__ void __launch_bounds__(kStepThreads, 6) step_learned_warp_kernel(cons
         if (!(r > 0.f && r < 1.0e30f)) atomicOr(p.health, 1u);
       }
       store_cell_as<A>(p.ri, cell, f);
-      capture_cell(p.cap, cell, f);
     }
   }
 }

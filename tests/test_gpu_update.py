@@ -1,17 +1,13 @@
-"""The update kernel on arbitrary shifts, the per-cell Smagorinsky hook, and the
-coarse/fine restriction's capture.
+"""The update kernel on arbitrary shifts and the per-cell Smagorinsky hook.
 
 * Grids and shifts that exercise the shifted addressing -- one 128-cell block, several
   blocks with a partial last one, shifts whose wrap point falls inside a block or between
-  the two cells of a pair (the 16-bit forms' pair kernel), an odd cell count (one cell per
-  thread), arbitrary shifts -- for every storage form, with and without a per-cell C_s
+  the two cells of a pair, an odd cell count, arbitrary shifts -- for every storage form, with and without a per-cell C_s
   field, with skipped and solid cells among the fluid ones: every cell against the
   oracle's collision (FP64), skipped cells unchanged and solid cells bounced back bit for
   bit.
 * A refined LES sphere run whose coarse grid has a per-cell C_s (a sponge ahead of the
   outlet, getSmagorinskyConstant per cell) against the reference's own update run live.
-* The x-face ring cells restricted from the fine update's capture against the restriction
-  that reads the fine grid: bit for bit.
 """
 import numpy as np
 import pytest
@@ -103,44 +99,3 @@ def test_per_cell_smagorinsky_sphere_matches_reference(ref):
     g.close()
     r.close()
 
-
-def _update(grids, level, invalidate):
-    """updateGrid (flowAroundSphereMainSingle.cu:158-167); with `invalidate` every fine grid's
-    capture is made stale before its transfer (re-setting the shifts counts as a change), so
-    the restriction reads the fine grid itself."""
-    from periodicshiftlbm_b200 import applyCoarseFineGridCommunication, applyStreaming
-
-    g = grids[level]
-    applyStreaming(g)
-    applyLocalCellUpdate(g)
-    if level < len(grids) - 1:
-        _update(grids, level + 1, invalidate)
-        _update(grids, level + 1, invalidate)
-        if invalidate:
-            grids[level + 1].shifter = grids[level + 1].shifter
-        applyCoarseFineGridCommunication(g, grids[level + 1])
-
-
-@pytest.mark.parametrize("storage,closure", [("f32", False), ("f16", False), ("bf16", False), ("f16", True)])
-def test_restriction_from_capture_equals_direct_reads(storage, closure):
-    """The x-face ring cells restricted from the fine update's capture give the bits of the
-    restriction that reads the fine grid (three levels: both transfers use it)."""
-    case = SphereCase(nx=32, ny=16, nz=16, sphere=(12.0, 9.0, 9.0), radius=1.5, nu=0.004, smagorinsky=0.1,
-                      refine=((6, 4, 4), (18, 12, 12)), refine2=((6, 6, 6), (18, 14, 14)))
-    a, b = GpuSim(case, storage=storage), GpuSim(case, storage=storage)
-    if closure:
-        from oracle import mlp_oracle as mo
-        from periodicshiftlbm_b200.sgs import set_sgs_mlp
-
-        p = mo.random_params(2)
-        for s in (a, b):
-            for g in s.grids:
-                set_sgs_mlp(g, p, g.Info.res / s.grids[0].Info.res)
-    for _ in range(6):
-        _update(a.grids, 0, False)
-        _update(b.grids, 0, True)
-    for lev in range(3):
-        assert np.array_equal(a.populations(lev), b.populations(lev)), lev
-        assert a.grids[lev].health() == 0
-    a.close()
-    b.close()

@@ -82,6 +82,16 @@ typedef struct psl_sphere_case {
 /* ---- grid lifetime (replaces GridStruct construction, fArray.setSizes(27, N) and
  *      shifter = IntArrayType(27, 0): flowAroundSphereMainSingle.cu:171-182) ---- */
 int psl_grid_create(const psl_info* info, int storage, psl_grid** out);
+/* The population rows are mapped twice back to back in virtual memory when the row size is a
+ * multiple of the driver's mapping granularity (2 MiB: 1,048,576 cells in FP16/BF16,
+ * 524,288 in FP32) and 55 N < 2^32, so the update addresses cell + shift without the
+ * periodic wrap; other grids, and grids made with PSL_GRID_ONE_MAPPING, use one plain
+ * allocation.  Results are the same bits either way. */
+#define PSL_GRID_ONE_MAPPING 1u
+int psl_grid_create_ex(const psl_info* info, int storage, unsigned int flags, psl_grid** out);
+/* rows_mapped_twice: 1 when the rows are mapped twice; row_stride: elements from one
+ * population row to the next (2N when mapped twice). */
+int psl_grid_get_layout(const psl_grid* grid, int* rows_mapped_twice, long long* row_stride);
 int psl_grid_destroy(psl_grid* grid);
 int psl_grid_set_stream(psl_grid* grid, void* cuda_stream);
 int psl_grid_get_info(const psl_grid* grid, psl_info* info, long long* cell_count, int* storage);

@@ -80,6 +80,10 @@ _lib = None
 # name -> (restype, argtypes); every entry point of include/psl.h
 _SIGNATURES = {
     "psl_grid_create": (ctypes.c_int, [ctypes.POINTER(PslInfo), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "psl_grid_create_ex": (ctypes.c_int, [ctypes.POINTER(PslInfo), ctypes.c_int, ctypes.c_uint,
+                                          ctypes.POINTER(ctypes.c_void_p)]),
+    "psl_grid_get_layout": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(ctypes.c_longlong)]),
     "psl_grid_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "psl_grid_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_grid_get_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PslInfo), ctypes.POINTER(ctypes.c_longlong),

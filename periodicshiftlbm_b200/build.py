@@ -28,7 +28,8 @@ NVCC_FLAGS = [
 SOURCES = [os.path.join(CSRC, "psl_capi.cu"), os.path.join(CSRC, "psl_noalloc.cu"), os.path.join(CSRC, "psl_batch.cu"),
            os.path.join(CSRC, "psl_learned.cu"),
            os.path.join(CSRC, "psl_train.cu"),
-           os.path.join(CSRC, "psl_reports.cu")]
+           os.path.join(CSRC, "psl_reports.cu"),
+           os.path.join(CSRC, "psl_rowmap.cu")]
 
 
 def _nvcc() -> str:

@@ -102,7 +102,7 @@ int upload_table(psl_batch* b) {
     c.rx.omega0 = 1.f / c.rx.tau;
     c.rx.cs18 = 18.f * g->cs;
     c.n = g->n;
-    c.stride = (uint32_t)g->stride;
+    c.stride = (uint32_t)g->f_stride;
     for (int q = 0; q < 27; ++q) {
       c.shift0[q] = b->shift0[i][q];
       c.adv[q] = b->adv[i][q];
@@ -236,7 +236,7 @@ int psl_batch_create(psl_grid* const* grids, int count, psl_batch** out) {
     BATCH_CHECK(g->storage != kStoreF64, PSL_ERR_INVALID, "psl_batch_create: FP64 storage is for oracle runs only");
     BATCH_CHECK(g->info.i_subgrid_end <= g->info.i_subgrid_start, PSL_ERR_INVALID,
                 "psl_batch_create: grids with a refinement block are not batched");
-    BATCH_CHECK(27ull * g->stride + g->n < (1ull << 32), PSL_ERR_INVALID, "psl_batch_create: grid too large");
+    BATCH_CHECK(27ull * g->f_stride + g->n < (1ull << 32), PSL_ERR_INVALID, "psl_batch_create: grid too large");
     BATCH_CHECK(!g->cs_field, PSL_ERR_INVALID,
                 "psl_batch_create: grids with a per-cell Smagorinsky field are not batched");
   }
@@ -353,9 +353,12 @@ int psl_batch_autotune(psl_batch* b, int trial_steps, psl_batch_tuning* chosen) 
   };
   for (size_t i = 0; i < b->grids.size(); ++i) {
     const psl_grid* g = b->grids[i];
-    bytes[i] = 27 * g->stride * storage_bytes(g->storage);
-    cudaError_t e = cudaMalloc(&saved[i], bytes[i]);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(saved[i], g->f, bytes[i], cudaMemcpyDeviceToDevice, b->stream);
+    // rows of N values each (f's rows may be mapped twice: copy one mapping)
+    bytes[i] = (size_t)g->n * storage_bytes(g->storage);
+    cudaError_t e = cudaMalloc(&saved[i], 27 * bytes[i]);
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(saved[i], bytes[i], g->f, g->f_stride * storage_bytes(g->storage), bytes[i], 27,
+                            cudaMemcpyDeviceToDevice, b->stream);
     if (e != cudaSuccess) {
       cudaGetLastError();
       release();
@@ -401,7 +404,8 @@ int psl_batch_autotune(psl_batch* b, int trial_steps, psl_batch_tuning* chosen) 
   cudaEventDestroy(t1);
   // restore the state and the counter, then adopt the winner
   for (size_t i = 0; i < b->grids.size(); ++i)
-    cudaMemcpyAsync(b->grids[i]->f, saved[i], bytes[i], cudaMemcpyDeviceToDevice, b->stream);
+    cudaMemcpy2DAsync(b->grids[i]->f, b->grids[i]->f_stride * storage_bytes(b->grids[i]->storage), saved[i], bytes[i],
+                      bytes[i], 27, cudaMemcpyDeviceToDevice, b->stream);
   cudaMemcpyAsync(b->step, &b->steps_done, sizeof(unsigned long long), cudaMemcpyHostToDevice, b->stream);
   cudaError_t e = cudaStreamSynchronize(b->stream);
   release();

@@ -14,6 +14,7 @@
 #include "psl.h"
 #include "psl_internal.h"
 #include "psl_kernels.cuh"
+#include "psl_rowmap.h"
 
 using namespace psl;
 
@@ -48,21 +49,21 @@ static GridView<S> view(const psl_grid* g) {
   GridView<S> v;
   typename S::type* base = static_cast<typename S::type*>(g->f);
   for (int q = 0; q < 27; ++q) {
-    v.fq[q] = base + (size_t)q * g->stride;
+    v.fq[q] = base + (size_t)q * g->f_stride;
     v.shift[q] = g->shift[q];
   }
   v.n = g->n;
   return v;
 }
 
-// Base pointer + 32-bit row offsets of a grid (needs 27 * stride + N < 2^32).
+// Base pointer + 32-bit row offsets of a grid's populations (needs 27 f_stride + N < 2^32).
 template <typename S>
 static RowIndex<S> row_index(const psl_grid* g) {
   RowIndex<S> r;
   r.base = static_cast<typename S::type*>(g->f);
   r.n = g->n;
   for (int q = 0; q < 27; ++q) {
-    r.off[q] = (uint32_t)((size_t)q * g->stride + g->shift[q]);
+    r.off[q] = (uint32_t)((size_t)q * g->f_stride + g->shift[q]);
     r.lim[q] = g->n - g->shift[q];
   }
   return r;
@@ -125,7 +126,12 @@ const char* psl_last_error(void) { return g_last_error.c_str(); }
 const char* psl_version(void) { return "periodicshiftlbm_b200 0.1 (sm_100a)"; }
 
 int psl_grid_create(const psl_info* info, int storage, psl_grid** out) {
+  return psl_grid_create_ex(info, storage, 0u, out);
+}
+
+int psl_grid_create_ex(const psl_info* info, int storage, unsigned int flags, psl_grid** out) {
   PSL_CHECK(info && out, PSL_ERR_INVALID, "psl_grid_create: null argument");
+  PSL_CHECK((flags & ~(unsigned int)PSL_GRID_ONE_MAPPING) == 0, PSL_ERR_INVALID, "psl_grid_create: unknown flags");
   *out = nullptr;
   const long long nx = info->cell_count_x, ny = info->cell_count_y, nz = info->cell_count_z;
   PSL_CHECK(nx > 0 && ny > 0 && nz > 0, PSL_ERR_INVALID, "psl_grid_create: cell counts must be positive");
@@ -150,14 +156,27 @@ int psl_grid_create(const psl_info* info, int storage, psl_grid** out) {
   g->storage = storage;
   g->stride = ((size_t)n + 63) / 64 * 64;
   cudaGetDevice(&g->device);
-  const size_t bytes = 27 * g->stride * storage_bytes(storage);
-  cudaError_t e = cudaMalloc(&g->f, bytes);
+  const size_t elem = storage_bytes(storage);
+  // population rows mapped twice where the row size allows it (psl_rowmap.cu), else one
+  // allocation of 27 rows of `stride` elements
+  cudaError_t e = cudaErrorNotSupported;
+  const bool flat_fits = 55ull * (unsigned long long)n < (1ull << 32);  // 32-bit offsets of 27 rows of 2N, + N
+  if (!(flags & PSL_GRID_ONE_MAPPING) && flat_fits)
+    e = psl_row_map_create(g->device, (size_t)n * elem, 27, &g->f, &g->f_map, nullptr);
+  if (e == cudaSuccess) {
+    g->f_twice = true;
+    g->f_stride = 2 * (size_t)n;
+  } else {
+    cudaGetLastError();
+    g->f_stride = g->stride;
+    e = cudaMalloc(&g->f, 27 * g->stride * elem);
+  }
   if (e == cudaSuccess) e = cudaMalloc(&g->marker, g->stride);
   if (e == cudaSuccess) e = cudaMalloc(&g->health, 4 * sizeof(unsigned int));
   if (e == cudaSuccess) e = cudaMalloc(&g->scratch, (kForceBlocks * 3 + 3) * sizeof(double));
   if (e == cudaSuccess) e = cudaMemset(g->marker, make_marker(kFluid, 0), g->stride);
   if (e == cudaSuccess) e = cudaMemset(g->health, 0, 4 * sizeof(unsigned int));
-  if (e == cudaSuccess) e = cudaMemset(g->f, 0, bytes);
+  if (e == cudaSuccess) e = cudaMemset2D(g->f, g->f_stride * elem, 0, (g->f_twice ? (size_t)n : g->stride) * elem, 27);
   if (e != cudaSuccess) {
     const std::string msg = std::string("psl_grid_create: ") + cudaGetErrorString(e);
     psl_grid_destroy(g);
@@ -172,7 +191,8 @@ int psl_grid_destroy(psl_grid* g) {
   if (!g) return PSL_OK;
   PSL_CHECK(g->batched == 0, PSL_ERR_INVALID, "psl_grid_destroy: the grid belongs to a live batch");
   DeviceGuard dg(g->device);
-  if (g->f) cudaFree(g->f);
+  if (g->f_map) psl_row_map_destroy(g->f_map);
+  else if (g->f) cudaFree(g->f);
   if (g->marker) cudaFree(g->marker);
   if (g->given) cudaFree(g->given);
   if (g->health) cudaFree(g->health);
@@ -182,6 +202,13 @@ int psl_grid_destroy(psl_grid* g) {
   if (g->givenT) cudaFree(g->givenT);
   if (g->cs_field) cudaFree(g->cs_field);
   delete g;
+  return PSL_OK;
+}
+
+int psl_grid_get_layout(const psl_grid* g, int* rows_mapped_twice, long long* row_stride) {
+  PSL_CHECK(g, PSL_ERR_INVALID, "psl_grid_get_layout: null grid");
+  if (rows_mapped_twice) *rows_mapped_twice = g->f_twice ? 1 : 0;
+  if (row_stride) *row_stride = (long long)g->f_stride;
   return PSL_OK;
 }
 
@@ -489,17 +516,19 @@ static cudaError_t launch_step(psl_grid* g) {
   p.cs = g->cs_field;
   p.rx = relaxation<typename S::calc>(g);
   p.health = g->health;
-  p.ri.base = static_cast<typename S::type*>(g->f);
-  p.ri.n = g->n;
-  for (int q = 0; q < 27; ++q) {
-    p.ri.off[q] = (uint32_t)((size_t)q * g->stride + g->shift[q]);
-    p.ri.lim[q] = g->n - g->shift[q];
+  p.ri = row_index<S>(g);
+  const unsigned int blocks = blocks_for(g->n, kStepThreads);
+  const int addr = 27 * g->f_stride + g->n >= (1ull << 32) ? kAddrView : g->f_twice ? kAddrFlat : kAddrIndex;
+  auto launch = [&](auto kernel) { kernel<<<blocks, kStepThreads, 0, g->stream>>>(p); };
+  if constexpr (kCollidesOnG<S>) {
+    if (addr == kAddrView) launch(step_kernel_g<S, kAddrView>);
+    else if (addr == kAddrFlat) launch(step_kernel_g<S, kAddrFlat>);
+    else launch(step_kernel_g<S, kAddrIndex>);
+  } else {
+    if (addr == kAddrView) launch(step_kernel<S, kAddrView>);
+    else if (addr == kAddrFlat) launch(step_kernel<S, kAddrFlat>);
+    else launch(step_kernel<S, kAddrIndex>);
   }
-  const bool row_index = 27 * g->stride + g->n < (1ull << 32);
-  if (row_index)
-    step_kernel<S, true><<<blocks_for(g->n, kStepThreads), kStepThreads, 0, g->stream>>>(p);
-  else
-    step_kernel<S, false><<<blocks_for(g->n, kStepThreads), kStepThreads, 0, g->stream>>>(p);
   return cudaGetLastError();
 }
 
@@ -511,7 +540,7 @@ int psl_apply_local_cell_update(psl_grid* g) {
     PSL_CHECK(!custom && !g->mlp, PSL_ERR_INVALID,
               "psl_apply_local_cell_update: scalar transport does not combine with forcing, moving walls or the "
               "learned closure");
-    PSL_CHECK(g->storage != kStoreF64 && 27ull * g->stride + g->n < (1ull << 32), PSL_ERR_INVALID,
+    PSL_CHECK(g->storage != kStoreF64 && 27ull * g->f_stride + g->n < (1ull << 32) && 27ull * g->stride + g->n < (1ull << 32), PSL_ERR_INVALID,
               "psl_apply_local_cell_update: scalar transport needs FP32/FP16/BF16 storage");
     with_storage(g->storage, [&](auto s) {
       using S = decltype(s);
@@ -527,8 +556,8 @@ int psl_apply_local_cell_update(psl_grid* g) {
         sp.base.health = g->health;
         sp.T.base = g->T;
         sp.T.n = g->n;
-        for (int q = 0; q < 27; ++q) {
-          sp.T.off[q] = sp.base.ri.off[q];
+        for (int q = 0; q < 27; ++q) {  // the scalar rows: one plain allocation of row stride `stride`
+          sp.T.off[q] = (uint32_t)((size_t)q * g->stride + g->shift[q]);
           sp.T.lim[q] = sp.base.ri.lim[q];
         }
         sp.givenT = g->givenT;
@@ -546,7 +575,7 @@ int psl_apply_local_cell_update(psl_grid* g) {
     return psl_detail_launch_learned(g);
   }
   if (custom) {
-    PSL_CHECK(g->storage != kStoreF64 && 27ull * g->stride + g->n < (1ull << 32), PSL_ERR_INVALID,
+    PSL_CHECK(g->storage != kStoreF64 && 27ull * g->f_stride + g->n < (1ull << 32), PSL_ERR_INVALID,
               "psl_apply_local_cell_update: forcing and moving walls need FP32/FP16/BF16 storage");
     with_storage(g->storage, [&](auto s) {
       using S = decltype(s);
@@ -676,7 +705,7 @@ int psl_fill_coarse_grid_from_fine(psl_grid* c, psl_grid* f) {
   PSL_CHECK(F.cell_count_x == 2 * a && F.cell_count_y == 2 * b && F.cell_count_z == 2 * cc, PSL_ERR_INVALID,
             "fill coarse: fine grid is not twice the refinement block");
   PSL_CHECK(c->device == f->device, PSL_ERR_INVALID, "fill coarse: grids on different devices");
-  PSL_CHECK(27ull * c->stride + c->n < (1ull << 32) && 27ull * f->stride + f->n < (1ull << 32), PSL_ERR_INVALID,
+  PSL_CHECK(27ull * c->f_stride + c->n < (1ull << 32) && 27ull * f->f_stride + f->n < (1ull << 32), PSL_ERR_INVALID,
             "fill coarse: grid too large for 32-bit row offsets");
   DeviceGuard dg(c->device);
   return with_storage(c->storage, [&](auto s) { return launch_fill_coarse<decltype(s)>(c, f); });
@@ -694,7 +723,7 @@ int psl_apply_coarse_fine_grid_communication(psl_grid* c, psl_grid* f) {
   PSL_CHECK(F.cell_count_x == 2 * a && F.cell_count_y == 2 * b && F.cell_count_z == 2 * cc, PSL_ERR_INVALID,
             "coarse/fine: fine grid is not twice the refinement block");
   PSL_CHECK(c->device == f->device, PSL_ERR_INVALID, "coarse/fine: grids on different devices");
-  PSL_CHECK(27ull * c->stride + c->n < (1ull << 32) && 27ull * f->stride + f->n < (1ull << 32), PSL_ERR_INVALID,
+  PSL_CHECK(27ull * c->f_stride + c->n < (1ull << 32) && 27ull * f->f_stride + f->n < (1ull << 32), PSL_ERR_INVALID,
             "coarse/fine: grid too large for 32-bit row offsets");
   DeviceGuard dg(c->device);
   return with_storage(c->storage, [&](auto s) { return launch_coarse_fine<decltype(s)>(c, f); });

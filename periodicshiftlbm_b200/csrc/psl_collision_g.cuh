@@ -25,19 +25,42 @@
 // are subtracted inside the last pass, so the output is g' = f' - w.
 //
 // Same physics as collide<false> (psl_collision.cuh); results agree to FP32 rounding (the
-// operation order differs).  Templated on the arithmetic type (float everywhere today;
-// host-compilable, PSL_HDI, so the CPU tests can check it against the oracle's collision).
+// operation order differs, and the device takes the approximate reciprocal and square
+// root).  Templated on the arithmetic type (float everywhere today; host-compilable,
+// PSL_HDI, so the CPU tests can check it against the oracle's collision).
 #pragma once
 #include <math.h>
+#if defined(__CUDACC__)
+#include <cuda_fp16.h>
+#endif
 
 #include "psl_lattice.cuh"
 
 namespace psl {
 
-// The scalar forms of the operations the templates use.
+// The scalar forms of the operations the templates use.  On the device the reciprocal and
+// the square root are the single-instruction approximations of PTX (rcp.approx, sqrt.approx:
+// relative error of order 2^-23, far below the 16-bit forms' storage rounding of 2^-11 /
+// 2^-8); host builds (the CPU checks of this header) divide and take sqrtf.
 PSL_HDI float gfma(float a, float b, float c) { return fmaf(a, b, c); }
-PSL_HDI float grecip(float a) { return 1.f / a; }
-PSL_HDI float gsqrt(float a) { return sqrtf(a); }
+PSL_HDI float grecip(float a) {
+#if defined(__CUDA_ARCH__)
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+  return r;
+#else
+  return 1.f / a;
+#endif
+}
+PSL_HDI float gsqrt(float a) {
+#if defined(__CUDA_ARCH__)
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+  return r;
+#else
+  return sqrtf(a);
+#endif
+}
 PSL_HDI bool all_zero(float a) { return a == 0.f; }
 PSL_HDI float sel_zero(float c, float if_zero, float other) { return c == 0.f ? if_zero : other; }
 PSL_HDI bool finite_density(float rho) { return rho > 0.f && rho < 1.0e30f; }
@@ -49,18 +72,10 @@ struct RawMomentsGT {
   T rg, jx, jy, jz, sxx, syy, szz, sxy, sxz, syz;
 };
 
+// The y and x stages from the z-line sums (z0: sum, z1: first moment, z2: second moment
+// along z of each (x, y) line).
 template <typename T>
-PSL_HDI RawMomentsGT<T> raw_moments_g(const T (&g)[27]) {
-  T z0[3][3], z1[3][3], z2[3][3];
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      const T a = g[slot(i, j, 0)], b = g[slot(i, j, 1)], c = g[slot(i, j, 2)];
-      z2[i][j] = c + a;
-      z0[i][j] = z2[i][j] + b;
-      z1[i][j] = c - a;
-    }
+PSL_HDI RawMomentsGT<T> raw_moments_from_z(const T (&z0)[3][3], const T (&z1)[3][3], const T (&z2)[3][3]) {
   T y00[3], y10[3], y20[3], y01[3], y11[3], y02[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
@@ -85,6 +100,62 @@ PSL_HDI RawMomentsGT<T> raw_moments_g(const T (&g)[27]) {
   return m;
 }
 
+template <typename T>
+PSL_HDI RawMomentsGT<T> raw_moments_g(const T (&g)[27]) {
+  T z0[3][3], z1[3][3], z2[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const T a = g[slot(i, j, 0)], b = g[slot(i, j, 1)], c = g[slot(i, j, 2)];
+      z2[i][j] = c + a;
+      z0[i][j] = z2[i][j] + b;
+      z1[i][j] = c - a;
+    }
+  return raw_moments_from_z(z0, z1, z2);
+}
+
+#if defined(__CUDACC__)
+// The same sums started from the stored 16-bit values.  add.f32.f16 / add.f32.bf16 (PTX,
+// sm_100) convert their 16-bit operand and add in FP32 as one instruction; the conversion
+// is exact, so every sum is the one raw_moments_g forms from the converted values, bit for
+// bit (c - a is formed as -(a - c), the same rounding).
+template <bool kBF16>
+__device__ __forceinline__ float bits_to_float(uint16_t v) {
+  if constexpr (kBF16) return __uint_as_float((uint32_t)v << 16);
+  else return __half2float(__ushort_as_half(v));
+}
+template <bool kBF16>
+__device__ __forceinline__ float add_bits(uint16_t a, float c) {
+  float r;
+  if constexpr (kBF16) asm("add.rn.f32.bf16 %0, %1, %2;" : "=f"(r) : "h"(a), "f"(c));
+  else asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(r) : "h"(a), "f"(c));
+  return r;
+}
+template <bool kBF16>
+__device__ __forceinline__ float sub_bits(uint16_t a, float c) {
+  float r;
+  if constexpr (kBF16) asm("sub.rn.f32.bf16 %0, %1, %2;" : "=f"(r) : "h"(a), "f"(c));
+  else asm("sub.rn.f32.f16 %0, %1, %2;" : "=f"(r) : "h"(a), "f"(c));
+  return r;
+}
+template <bool kBF16>
+__device__ __forceinline__ RawMomentsGT<float> raw_moments_g_bits(const uint16_t (&h)[27]) {
+  float z0[3][3], z1[3][3], z2[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const uint16_t a = h[slot(i, j, 0)], b = h[slot(i, j, 1)];
+      const float c = bits_to_float<kBF16>(h[slot(i, j, 2)]);
+      z2[i][j] = add_bits<kBF16>(a, c);
+      z0[i][j] = add_bits<kBF16>(b, z2[i][j]);
+      z1[i][j] = -sub_bits<kBF16>(a, c);
+    }
+  return raw_moments_from_z(z0, z1, z2);
+}
+#endif
+
 // Density, velocity and D (second-order central moments less rho/3 I) of a cell.
 template <typename T>
 struct CellMomentsGT {
@@ -94,8 +165,7 @@ struct CellMomentsGT {
 using CellMomentsG = CellMomentsGT<float>;
 
 template <typename T>
-PSL_HDI CellMomentsGT<T> cell_moments_g(const T (&g)[27]) {
-  const RawMomentsGT<T> r = raw_moments_g(g);
+PSL_HDI CellMomentsGT<T> cell_moments_from_raw(const RawMomentsGT<T>& r) {
   CellMomentsGT<T> m;
   m.rho = T(1.f) + r.rg;
   m.inv_rho = grecip(m.rho);
@@ -110,6 +180,10 @@ PSL_HDI CellMomentsGT<T> cell_moments_g(const T (&g)[27]) {
   m.dxz = gfma(-r.jx, m.uz, r.sxz);
   m.dyz = gfma(-r.jy, m.uz, r.syz);
   return m;
+}
+template <typename T>
+PSL_HDI CellMomentsGT<T> cell_moments_g(const T (&g)[27]) {
+  return cell_moments_from_raw(raw_moments_g(g));
 }
 
 // Smagorinsky rate from D (include/cellFunctions.h:157-198): 1/tau without LES, else

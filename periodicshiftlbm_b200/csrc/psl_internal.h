@@ -33,7 +33,11 @@ struct psl_grid {
   psl_info info;
   uint32_t n = 0;
   int storage = 0;
-  size_t stride = 0;  // elements per population row, multiple of 64 (128-byte rows)
+  size_t stride = 0;    // elements per per-cell array (markers, C_s, scalar rows): N rounded up to 64
+  size_t f_stride = 0;  // elements from one population row of f to the next
+  bool f_twice = false; // each population row mapped twice (psl_rowmap.cu): f_stride = 2N and
+                        // row element N + i is element i, so the update needs no wrap
+  struct psl_row_map* f_map = nullptr;  // the mappings when f_twice, else f is one cudaMalloc
   void* f = nullptr;
   uint8_t* marker = nullptr;
   float4* given = nullptr;

@@ -170,6 +170,22 @@ template <typename S>
 __device__ __forceinline__ void store_cell(const GridView<S>& g, uint32_t cell, const typename S::calc (&f)[27]) {
   store_cell_as<S>(g, cell, f);
 }
+// Rows mapped twice (psl_rowmap.cu): cell + off_q < row start + 2N addresses the wrapped
+// element through the row's second mapping, so no wrap compare.
+template <typename A, typename S, int Q = 0>
+__device__ __forceinline__ void load_cell_flat(const RowIndex<S>& r, uint32_t cell, typename A::calc (&f)[27]) {
+  if constexpr (Q < 27) {
+    f[Q] = A::template load_once<Q>(r.base + (cell + r.off[Q]));
+    load_cell_flat<A, S, Q + 1>(r, cell, f);
+  }
+}
+template <typename A, typename S, int Q = 0>
+__device__ __forceinline__ void store_cell_flat(const RowIndex<S>& r, uint32_t cell, const typename A::calc (&f)[27]) {
+  if constexpr (Q < 27) {
+    A::template store_once<Q>(r.base + (cell + r.off[Q]), f[Q]);
+    store_cell_flat<A, S, Q + 1>(r, cell, f);
+  }
+}
 template <typename S>
 __device__ __forceinline__ void load_cell_ri(const RowIndex<S>& r, uint32_t cell, typename S::calc (&f)[27]) {
   load_cell_as<S>(r, cell, f);
@@ -202,39 +218,40 @@ __device__ __forceinline__ void local_cell_update(int kind, uint8_t m, T (&f)[27
   }
 }
 
-template <typename S, bool kRowIndex>
-__device__ __forceinline__ void load_for(const StepParams<S>& p, uint32_t cell, typename S::calc (&f)[27]) {
-  using A = StoredOf<S>;
-  if constexpr (kRowIndex) load_cell_as<A>(p.ri, cell, f);
+// Population addressing of the update kernels:
+//   kAddrView   64-bit row pointers with the periodic wrap (GridView)
+//   kAddrIndex  base + 32-bit row offsets with the wrap (RowIndex; 27 rows + N < 2^32 elements)
+//   kAddrFlat   base + 32-bit row offsets without the wrap, on rows mapped twice
+enum RowAddr : int { kAddrView = 0, kAddrIndex = 1, kAddrFlat = 2 };
+
+template <typename A, int kAddr, typename S>
+__device__ __forceinline__ void load_for(const StepParams<S>& p, uint32_t cell, typename A::calc (&f)[27]) {
+  if constexpr (kAddr == kAddrFlat) load_cell_flat<A>(p.ri, cell, f);
+  else if constexpr (kAddr == kAddrIndex) load_cell_as<A>(p.ri, cell, f);
   else load_cell_as<A>(p.g, cell, f);
 }
-template <typename S, bool kRowIndex>
-__device__ __forceinline__ void store_for(const StepParams<S>& p, uint32_t cell, const typename S::calc (&f)[27]) {
-  using A = StoredOf<S>;
-  if constexpr (kRowIndex) store_cell_as<A>(p.ri, cell, f);
+template <typename A, int kAddr, typename S>
+__device__ __forceinline__ void store_for(const StepParams<S>& p, uint32_t cell, const typename A::calc (&f)[27]) {
+  if constexpr (kAddr == kAddrFlat) store_cell_flat<A>(p.ri, cell, f);
+  else if constexpr (kAddr == kAddrIndex) store_cell_as<A>(p.ri, cell, f);
   else store_cell_as<A>(p.g, cell, f);
 }
-// The update of one cell (applyLocalCellUpdate.h:21-72).  The 16-bit forms load and store
-// their stored values g = f - w and collide on them (collide_cell_g); FP32 and FP64 run
-// collide<false> on f, the reference's operation order.  `slot`: the thread's shared-memory
-// slot for the boundary functions.
-template <typename S, bool kRowIndex>
-__device__ __forceinline__ void update_one_cell(const StepParams<S>& p, uint32_t cell, uint8_t m, float* slot) {
+// The update of one cell (applyLocalCellUpdate.h:21-72) for FP32 and FP64 storage:
+// collide<false> on f, the reference's operation order.
+template <typename S, int kAddr>
+__device__ __forceinline__ void update_one_cell(const StepParams<S>& p, uint32_t cell, uint8_t m) {
   const int kind = marker_kind(m);
+  if (kind == kSkip) return;
   using T = typename S::calc;
   T f[27];
-  if (kind == kSkip) return;
-  load_for<S, kRowIndex>(p, cell, f);
-  if (kind == kSolid) {  // bounce-back: g and f swap alike (w_q = w_opposite(q))
+  load_for<StoredOf<S>, kAddr>(p, cell, f);
+  if (kind == kSolid) {
 #pragma unroll
     for (int q = 1; q < 27; q += 2) {
       const T t = f[q];
       f[q] = f[q + 1];
       f[q + 1] = t;
     }
-  } else if constexpr (kCollidesOnG<S>) {
-    collide_cell_g(kind, m, f, p.given, p.given_uniform, cell, p.rx, p.cs ? 18.f * p.cs[cell] : p.rx.cs18, p.health,
-                   slot);
   } else {
     if (kind != kFluid) apply_boundary(m, f, p.given ? p.given[cell] : p.given_uniform);
     collide<false>(f, cell_relaxation(p.rx, p.cs, cell));
@@ -243,20 +260,78 @@ __device__ __forceinline__ void update_one_cell(const StepParams<S>& p, uint32_t
       if (!(r > T(0) && r < T(1.0e30))) atomicOr(p.health, 1u);
     }
   }
-  store_for<S, kRowIndex>(p, cell, f);
+  store_for<StoredOf<S>, kAddr>(p, cell, f);
 }
 
-// One thread per cell.
-template <typename S, bool kRowIndex>
+// The same for the 16-bit forms, on their stored bits g = f - w (applyLocalCellUpdate.h:
+// 21-72): solid cells swap the bits; fluid cells start the moment sums from them
+// (raw_moments_g_bits); boundary cells go through f = g + w for the boundary functions; all
+// collide on g (psl_collision_g.cuh), bitwise as collide_cell_g on the converted values.
+// `slot`: the thread's shared-memory slot for the boundary functions.  Written for the
+// register allocator: the collided cells' loads and stores are predicated on one flag
+// instead of sitting behind early returns (which cost ~50 spilled registers at the 64-register
+// cap), and lanes that do not collide run the arithmetic on zeros.  `cell` must be < N.
+template <typename S, int kAddr>
+__device__ __forceinline__ void update_one_cell_g(const StepParams<S>& p, uint32_t cell, uint8_t m, float* slot) {
+  using B = StoredBits<S>;
+  const int kind = marker_kind(m);
+  uint16_t h[27];
+  if (kind == kSolid) {  // bounce-back: g and f swap alike (w_q = w_opposite(q))
+    load_for<B, kAddr>(p, cell, h);
+#pragma unroll
+    for (int q = 1; q < 27; q += 2) {
+      const uint16_t t = h[q];
+      h[q] = h[q + 1];
+      h[q + 1] = t;
+    }
+    store_for<B, kAddr>(p, cell, h);
+  }
+  const bool collides = kind != kSkip && kind != kSolid;
+  if (collides) {
+    load_for<B, kAddr>(p, cell, h);
+  } else {
+#pragma unroll
+    for (int q = 0; q < 27; ++q) h[q] = 0;
+  }
+  float g[27];
+  CellMomentsG cm;
+  if (!collides || kind == kFluid) {
+    cm = cell_moments_from_raw(raw_moments_g_bits<S::kind == kStoreBF16>(h));
+  } else {
+#pragma unroll
+    for (int q = 0; q < 27; ++q) g[q] = B::to_float(h[q]) + lattice_weight(q);
+    apply_boundary_at(m, g, p.given ? p.given[cell] : p.given_uniform, slot);
+#pragma unroll
+    for (int q = 0; q < 27; ++q) g[q] -= lattice_weight(q);
+    cm = cell_moments_g(g);
+  }
+  if (collides && p.health && !finite_density(cm.rho)) atomicOr(p.health, 1u);
+  const float cs18 = collides && p.cs ? 18.f * p.cs[cell] : p.rx.cs18;
+  relax_rebuild_g(g, cm, smagorinsky_omega_g(cm, p.rx.omega0, p.rx.tau, p.rx.tau2, cs18));
+  if (collides) store_for<StoredOf<S>, kAddr>(p, cell, g);
+}
+
+// One thread per cell: FP32 / FP64 storage.
+template <typename S, int kAddr>
 __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constant__ StepParams<S> p) {
+  static_assert(!kCollidesOnG<S>, "16-bit storage runs step_kernel_g");
   const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
   if (cell >= p.g.n) return;
-  if constexpr (kCollidesOnG<S>) {
-    __shared__ float slot[kStepThreads][27];
-    update_one_cell<S, kRowIndex>(p, cell, p.marker[cell], slot[threadIdx.x]);
-  } else {
-    update_one_cell<S, kRowIndex>(p, cell, p.marker[cell], nullptr);
-  }
+  update_one_cell<S, kAddr>(p, cell, p.marker[cell]);
+}
+
+// One thread per cell: the 16-bit forms, held to 64 registers (8 blocks of 128 per SM;
+// 4 with 64-bit row pointers).  Left free the compiler hoists loads into 96 registers and
+// the lower occupancy costs more than the hoisting gains.
+template <typename S, int kAddr>
+__global__ void __launch_bounds__(kStepThreads, kAddr == kAddrView ? 4 : 8) step_kernel_g(const __grid_constant__ StepParams<S> p) {
+  static_assert(kCollidesOnG<S>, "FP32 / FP64 storage runs step_kernel");
+  __shared__ float slot[kStepThreads][27];
+  const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
+  const bool in = cell < p.g.n;
+  const uint8_t m = in ? p.marker[cell] : make_marker(kSkip, 0);
+  if (__all_sync(0xffffffffu, marker_kind(m) == kSkip)) return;  // ghost layers, refined interior
+  update_one_cell_g<S, kAddr>(p, in ? cell : 0u, m, slot[threadIdx.x]);
 }
 
 // ------------------------------------------------------------------------------------------

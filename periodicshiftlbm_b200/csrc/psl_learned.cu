@@ -107,12 +107,12 @@ int launch(psl_grid* g) {
   const MlpBoth* both = static_cast<const MlpBoth*>(g->mlp);
   MlpScalars sc;
   std::memcpy(&sc, g->mlp_scalars, sizeof(MlpScalars));
-  if (27ull * g->stride + g->n >= (1ull << 32)) return fail(PSL_ERR_INVALID, "learned update: grid too large");
+  if (27ull * g->f_stride + g->n >= (1ull << 32)) return fail(PSL_ERR_INVALID, "learned update: grid too large");
   LearnedParams<S> p;
   p.ri.base = static_cast<typename S::type*>(g->f);
   p.ri.n = g->n;
   for (int q = 0; q < 27; ++q) {
-    p.ri.off[q] = (uint32_t)((size_t)q * g->stride + g->shift[q]);
+    p.ri.off[q] = (uint32_t)((size_t)q * g->f_stride + g->shift[q]);
     p.ri.lim[q] = g->n - g->shift[q];
   }
   p.marker = g->marker;
@@ -124,7 +124,11 @@ int launch(psl_grid* g) {
   p.width = g->mlp_width;
   p.n = g->n;
   p.health = g->health;
-  step_learned_warp_kernel<S><<<(g->n + kStepThreads - 1) / kStepThreads, kStepThreads, 0, g->stream>>>(p);
+  const unsigned int blocks = (g->n + kStepThreads - 1) / kStepThreads;
+  if (g->f_twice)
+    step_learned_warp_kernel<S, true><<<blocks, kStepThreads, 0, g->stream>>>(p);
+  else
+    step_learned_warp_kernel<S, false><<<blocks, kStepThreads, 0, g->stream>>>(p);
   MLP_CUDA(cudaGetLastError());
   return PSL_OK;
 }

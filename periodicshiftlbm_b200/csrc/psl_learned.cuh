@@ -54,9 +54,21 @@ __device__ __forceinline__ void mlp_features_d(const CellMomentsG& m, float widt
 }
 
 // One thread per cell with the fused closure.  16-bit storage collides on its stored
-// g = f - w (only the ten moments live across the closure's MMAs); FP32 runs the plain FP32
-// update's operation order, only the rate differs.
-template <typename S>
+// g = f - w (only the ten moments live across the closure's MMAs), fluid cells starting the
+// moment sums from the stored bits; FP32 runs the plain FP32 update's operation order, only
+// the rate differs.  kFlat: rows mapped twice, addressed without the wrap.
+template <typename A, bool kFlat, typename S>
+__device__ __forceinline__ void load_rows(const RowIndex<S>& r, uint32_t cell, typename A::calc (&f)[27]) {
+  if constexpr (kFlat) load_cell_flat<A>(r, cell, f);
+  else load_cell_as<A>(r, cell, f);
+}
+template <typename A, bool kFlat, typename S>
+__device__ __forceinline__ void store_rows(const RowIndex<S>& r, uint32_t cell, const typename A::calc (&f)[27]) {
+  if constexpr (kFlat) store_cell_flat<A>(r, cell, f);
+  else store_cell_as<A>(r, cell, f);
+}
+
+template <typename S, bool kFlat>
 __global__ void __launch_bounds__(kStepThreads, 6) step_learned_warp_kernel(const __grid_constant__ LearnedParams<S> p) {
   __shared__ __align__(16) float bc_slot[kStepThreads][27];
   // the warp's FP16 feature tile lives in its own lanes' boundary slots (free after the
@@ -65,41 +77,57 @@ __global__ void __launch_bounds__(kStepThreads, 6) step_learned_warp_kernel(cons
   const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
   const uint8_t m = cell < p.n ? p.marker[cell] : make_marker(kSkip, 0);
   const int kind = marker_kind(m);
-  using A = StoredOf<S>;
   float x[kMlpIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   float f[27];
-  if (kind != kSkip) load_cell_as<A>(p.ri, cell, f);
-  if (kind == kSolid) {  // bounce-back: done before the closure, nothing to keep
-#pragma unroll
-    for (int q = 1; q < 27; q += 2) {
-      const float t = f[q];
-      f[q] = f[q + 1];
-      f[q + 1] = t;
-    }
-    store_cell_as<A>(p.ri, cell, f);
-  }
   const bool collides = kind != kSkip && kind != kSolid;
   if constexpr (kCollidesOnG<S>) {
+    using B = StoredBits<S>;
+    uint16_t h[27];
+    if (kind == kSolid) {  // bounce-back: done before the closure, nothing to keep
+      load_rows<B, kFlat>(p.ri, cell, h);
+#pragma unroll
+      for (int q = 1; q < 27; q += 2) {
+        const uint16_t t = h[q];
+        h[q] = h[q + 1];
+        h[q + 1] = t;
+      }
+      store_rows<B, kFlat>(p.ri, cell, h);
+    }
+    if (collides) load_rows<B, kFlat>(p.ri, cell, h);
     CellMomentsG cm{};
     if (collides) {
-      if (kind != kFluid) {
+      if (kind == kFluid) {
+        cm = cell_moments_from_raw(raw_moments_g_bits<S::kind == kStoreBF16>(h));
+      } else {
 #pragma unroll
-        for (int q = 0; q < 27; ++q) f[q] += lattice_weight(q);
+        for (int q = 0; q < 27; ++q) f[q] = B::to_float(h[q]) + lattice_weight(q);
         apply_boundary_at(m, f, p.given ? p.given[cell] : p.given_uniform, bc_slot[threadIdx.x]);
 #pragma unroll
         for (int q = 0; q < 27; ++q) f[q] -= lattice_weight(q);
+        cm = cell_moments_g(f);
       }
-      cm = cell_moments_g(f);
-      if (p.health && !(cm.rho > 0.f && cm.rho < 1.0e30f)) atomicOr(p.health, 1u);
+      if (p.health && !finite_density(cm.rho)) atomicOr(p.health, 1u);
       mlp_features_d(cm, p.width, x);
     }
     __syncwarp();
     const float nu_t = mlp_warp_eval(p.mlpw, p.sc, xt, x);
     if (collides) {
       relax_rebuild_g(f, cm, 1.f / (3.f * (p.nu + nu_t) + 0.5f));
-      store_cell_as<A>(p.ri, cell, f);
+      store_rows<StoredOf<S>, kFlat>(p.ri, cell, f);
     }
   } else {
+    using A = StoredOf<S>;
+    if (kind == kSolid) {  // bounce-back: done before the closure, nothing to keep
+      load_rows<A, kFlat>(p.ri, cell, f);
+#pragma unroll
+      for (int q = 1; q < 27; q += 2) {
+        const float t = f[q];
+        f[q] = f[q + 1];
+        f[q + 1] = t;
+      }
+      store_rows<A, kFlat>(p.ri, cell, f);
+    }
+    if (collides) load_rows<A, kFlat>(p.ri, cell, f);
     float K[3][3][3];
     float rho = 1.f, ux = 0.f, uy = 0.f, uz = 0.f, inv_rho = 1.f;
     if (collides) {
@@ -115,7 +143,7 @@ __global__ void __launch_bounds__(kStepThreads, 6) step_learned_warp_kernel(cons
         const float r = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6];
         if (!(r > 0.f && r < 1.0e30f)) atomicOr(p.health, 1u);
       }
-      store_cell_as<A>(p.ri, cell, f);
+      store_rows<A, kFlat>(p.ri, cell, f);
     }
   }
 }

@@ -58,7 +58,7 @@ GridView<S> view_of(const psl_grid* g) {
   GridView<S> v;
   typename S::type* base = static_cast<typename S::type*>(g->f);
   for (int q = 0; q < 27; ++q) {
-    v.fq[q] = base + (size_t)q * g->stride;
+    v.fq[q] = base + (size_t)q * g->f_stride;
     v.shift[q] = g->shift[q];
   }
   v.n = g->n;

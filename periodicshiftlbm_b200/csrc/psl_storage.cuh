@@ -131,6 +131,31 @@ struct StoredOf {
 template <typename S>
 constexpr bool kCollidesOnG = S::kind == kStoreF16 || S::kind == kStoreBF16;
 
+// The 16 stored bits of a 16-bit form, unconverted: the update's fluid cells feed them to
+// the moment sums directly (raw_moments_g_bits), solid cells swap them.
+template <typename S>
+struct StoredBits {
+  static_assert(kCollidesOnG<S>, "16-bit storage forms only");
+  using type = typename S::type;
+  using calc = uint16_t;
+  template <int Q>
+  __device__ __forceinline__ static uint16_t load_once(const type* p) {
+    return __ldg(reinterpret_cast<const unsigned short*>(p));
+  }
+  template <int Q>
+  __device__ __forceinline__ static void store_once(type* p, uint16_t v) {
+    __stcs(reinterpret_cast<unsigned short*>(p), v);
+  }
+  template <int Q>
+  __device__ __forceinline__ static uint16_t load(const type* p) { return *reinterpret_cast<const unsigned short*>(p); }
+  template <int Q>
+  __device__ __forceinline__ static void store(type* p, uint16_t v) { *reinterpret_cast<unsigned short*>(p) = v; }
+  __device__ __forceinline__ static float to_float(uint16_t v) {
+    if constexpr (S::kind == kStoreF16) return __half2float(__ushort_as_half(v));
+    else return __bfloat162float(__ushort_as_bfloat16(v));
+  }
+};
+
 inline size_t storage_bytes(int kind) { return kind == kStoreF32 ? 4 : kind == kStoreF64 ? 8 : 2; }
 
 }  // namespace psl

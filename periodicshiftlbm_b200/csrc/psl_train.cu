@@ -462,7 +462,7 @@ int psl_sgs_trainer_add_filtered(psl_sgs_trainer* t, psl_grid* fine, int M, int 
     GridView<S> v;
     typename S::type* base = static_cast<typename S::type*>(fine->f);
     for (int q = 0; q < 27; ++q) {
-      v.fq[q] = base + (size_t)q * fine->stride;
+      v.fq[q] = base + (size_t)q * fine->f_stride;
       v.shift[q] = fine->shift[q];
     }
     v.n = fine->n;

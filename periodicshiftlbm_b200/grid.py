@@ -114,11 +114,22 @@ class GridStruct:
     """One PS grid on the GPU (GridStruct, include/types.h:77): metadata, the [27][N]
     population array and the 27 periodic shifts.  Owns its device memory."""
 
-    def __init__(self, Info: InfoStruct, storage: str = "f32"):
+    def __init__(self, Info: InfoStruct, storage: str = "f32", one_mapping: bool = False):
+        """``one_mapping``: keep the population rows in one plain allocation even where they
+        could be mapped twice (psl.h, psl_grid_create_ex); the results are the same bits."""
         self.Info = Info
         self.storage = storage
         self._h = ctypes.c_void_p()
-        call("psl_grid_create", ctypes.byref(Info.to_c()), _lib.STORAGE[storage], ctypes.byref(self._h))
+        call("psl_grid_create_ex", ctypes.byref(Info.to_c()), _lib.STORAGE[storage],
+             ctypes.c_uint(1 if one_mapping else 0), ctypes.byref(self._h))
+
+    @property
+    def rows_mapped_twice(self) -> bool:
+        """Whether the population rows are mapped twice (the update then reads them without
+        the periodic wrap)."""
+        twice = ctypes.c_int()
+        call("psl_grid_get_layout", self._h, ctypes.byref(twice), None)
+        return bool(twice.value)
 
     @property
     def handle(self):

@@ -1,0 +1,80 @@
+"""Population rows mapped twice in virtual memory (psl_rowmap.cu).
+
+A grid whose row size is a whole number of the driver's mapping granularity maps every
+population row twice back to back, and the update kernels then read cell + shift without
+the periodic wrap.  Everything else about the grid is unchanged, so a grid made with
+PSL_GRID_ONE_MAPPING must give the same bits after any number of steps: the plain and the
+closure update, every storage form, arbitrary shifts (wrap points anywhere in the rows),
+a refined two-level run whose fine grid keeps one mapping.
+"""
+import numpy as np
+import pytest
+
+from periodicshiftlbm_b200 import GridStruct, InfoStruct, updateGrid
+from periodicshiftlbm_b200.cases import config2, make_sphere_grids
+from periodicshiftlbm_b200.grid import getSphereDrag
+from oracle import mlp_oracle as mo
+from periodicshiftlbm_b200.sgs import set_sgs_mlp
+
+pytestmark = pytest.mark.gpu
+
+MIB2 = 2 * 1024 * 1024
+
+
+@pytest.mark.parametrize("storage,dims,twice", [
+    ("f16", (128, 128, 64), True),     # 2 MiB rows
+    ("bf16", (256, 128, 64), True),    # 4 MiB
+    ("f32", (128, 64, 64), True),      # 2 MiB
+    ("f16", (128, 64, 64), False),     # 1 MiB: one mapping
+    ("f32", (127, 128, 64), False),    # not a whole number of 2 MiB
+])
+def test_layout(storage, dims, twice):
+    nx, ny, nz = dims
+    g = GridStruct(InfoStruct(cellCountX=nx, cellCountY=ny, cellCountZ=nz, nu=0.01), storage=storage)
+    assert g.rows_mapped_twice == twice
+    g1 = GridStruct(InfoStruct(cellCountX=nx, cellCountY=ny, cellCountZ=nz, nu=0.01), storage=storage,
+                    one_mapping=True)
+    assert not g1.rows_mapped_twice
+    g.close()
+    g1.close()
+
+
+def _random_shifts(n, seed):
+    rng = np.random.default_rng(seed)
+    s = rng.integers(0, n, 27)
+    s[1:5] = n - 1 - np.arange(4)      # wrap points at the start of the rows
+    s[5:8] = [1, 2, 127]               # and near their ends
+    s[0] = 0
+    return s.astype(np.int32)
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+@pytest.mark.parametrize("closure", [False, True])
+def test_twice_mapped_equals_one_mapping(storage, closure):
+    cfg = config2(scale=0.5)          # coarse 256x128x128: rows of 8 / 16 MiB, mapped twice
+    runs = []
+    for one in (False, True):
+        grids, case = make_sphere_grids(cfg, storage=storage, one_mapping=one)
+        assert grids[0].rows_mapped_twice == (not one)
+        assert not grids[1].rows_mapped_twice  # 128x96x96 fine cells: not a whole number of 2 MiB
+        sh = _random_shifts(grids[0].cellCount, 5)
+        f0 = grids[0].fArray
+        grids[0].shifter = sh
+        grids[0].fArray = f0      # the same logical state under the new shifts
+        if closure:
+            p = mo.random_params(11)
+            for g in grids:
+                set_sgs_mlp(g, p, filter_width=1.0)
+        drags = []
+        for _ in range(6):
+            updateGrid(grids, 0)
+            drags.append(getSphereDrag(grids[1], case))
+        runs.append((grids, [g.fArray for g in grids], [g.shifter for g in grids], drags))
+    (ga, fa, sa, da), (gb, fb, sb, db) = runs
+    for lvl in range(2):
+        assert np.array_equal(sa[lvl], sb[lvl])
+        assert np.array_equal(fa[lvl], fb[lvl]), (lvl, np.abs(fa[lvl] - fb[lvl]).max())
+    assert da == db
+    for g in ga + gb:
+        assert g.health() == 0
+        g.close()

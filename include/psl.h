@@ -180,6 +180,11 @@ int psl_update_grid(psl_grid** grids, int levels, int level);
  * the solid cells of the sphere's bounding box, lattice units of `grid`; force[0] is the
  * drag (x), force[1..2] the y and z components. */
 int psl_sphere_force(psl_grid* grid, const psl_sphere_case* sc, double* force3);
+/* The same without waiting: enqueued on the grid's stream, `force3` (device memory or pinned
+ * host memory, 3 doubles) holds the force once the stream has passed this point
+ * (psl_synchronize, or an event recorded after the call).  A step loop that keeps the drag
+ * of every step in a pinned host array reads it back every step and synchronises once. */
+int psl_sphere_force_async(psl_grid* grid, const psl_sphere_case* sc, double* force3);
 
 /* Torque (r x F, r = cell centre - point3, physical units of the grid) and force of the
  * momentum exchange summed over the solid cells of the box [lo3, hi3), FP64.  Counterpart

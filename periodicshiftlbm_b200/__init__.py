@@ -24,6 +24,7 @@ from .grid import (  # noqa: F401
     getFlowReport,
     getForcingTorque,
     getSphereForce,
+    getSphereForceAsync,
     getTorque,
     setBodyForce,
     setGivenRhoUxUyUz,

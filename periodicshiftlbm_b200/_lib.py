@@ -108,6 +108,7 @@ _SIGNATURES = {
     "psl_fill_coarse_grid_from_fine": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_update_grid": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int]),
     "psl_sphere_force": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PslSphereCase), ctypes.c_void_p]),
+    "psl_sphere_force_async": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PslSphereCase), ctypes.c_void_p]),
     "psl_momentum_exchange_force_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p,
                                                            ctypes.c_longlong, ctypes.c_void_p, ctypes.c_int,
                                                            ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,

@@ -753,9 +753,10 @@ static void launch_force(psl_grid* g, int i0, int j0, int k0, int si, int sj, in
                                                      g->info.cell_count_y, i0, j0, k0, si, sj, sk, g->scratch);
 }
 
-int psl_sphere_force(psl_grid* g, const psl_sphere_case* sc, double* force3) {
-  PSL_CHECK(g && sc && force3, PSL_ERR_INVALID, "psl_sphere_force: null argument");
-  DeviceGuard dg(g->device);
+// Enqueues the momentum-exchange force of the sphere's box on the grid's stream; the
+// result (3 doubles) lands in `force3` (device or pinned host memory) when the stream
+// reaches the copy.  Returns 1 with nothing enqueued when the box is empty.
+static int enqueue_sphere_force(psl_grid* g, const psl_sphere_case* sc, double* force3, cudaMemcpyKind kind) {
   const psl_info& I = g->info;
   // bounding box as getSphereDrag computes it (flowAroundSphereMainSingle.cu:105-110)
   int i0 = (int)((sc->sphere_x - sc->sphere_r - I.ox) / I.res);
@@ -766,8 +767,7 @@ int psl_sphere_force(psl_grid* g, const psl_sphere_case* sc, double* force3) {
   int k1 = (int)((sc->sphere_z + sc->sphere_r - I.oz) / I.res) + 2;
   i0 = std::max(i0, 0); j0 = std::max(j0, 0); k0 = std::max(k0, 0);
   i1 = std::min(i1, I.cell_count_x); j1 = std::min(j1, I.cell_count_y); k1 = std::min(k1, I.cell_count_z);
-  force3[0] = force3[1] = force3[2] = 0.0;
-  if (i1 <= i0 || j1 <= j0 || k1 <= k0) return PSL_OK;
+  if (i1 <= i0 || j1 <= j0 || k1 <= k0) return 1;
   const int si = i1 - i0, sj = j1 - j0, sk = k1 - k0;
   const int nb = (int)std::min<long long>(kForceBlocks, ((long long)si * sj * sk + 255) / 256);
   with_storage(g->storage, [&](auto s) {
@@ -776,9 +776,31 @@ int psl_sphere_force(psl_grid* g, const psl_sphere_case* sc, double* force3) {
   });
   force_final_kernel<<<1, 32, 0, g->stream>>>(g->scratch, nb, g->scratch + kForceBlocks * 3);
   PSL_CUDA(cudaGetLastError());
-  PSL_CUDA(cudaMemcpyAsync(force3, g->scratch + kForceBlocks * 3, 3 * sizeof(double), cudaMemcpyDeviceToHost, g->stream));
+  PSL_CUDA(cudaMemcpyAsync(force3, g->scratch + kForceBlocks * 3, 3 * sizeof(double), kind, g->stream));
+  return PSL_OK;
+}
+
+int psl_sphere_force(psl_grid* g, const psl_sphere_case* sc, double* force3) {
+  PSL_CHECK(g && sc && force3, PSL_ERR_INVALID, "psl_sphere_force: null argument");
+  DeviceGuard dg(g->device);
+  force3[0] = force3[1] = force3[2] = 0.0;
+  const int rc = enqueue_sphere_force(g, sc, force3, cudaMemcpyDeviceToHost);
+  if (rc == 1) return PSL_OK;
+  if (rc != PSL_OK) return rc;
   PSL_CUDA(cudaStreamSynchronize(g->stream));
   return PSL_OK;
+}
+
+int psl_sphere_force_async(psl_grid* g, const psl_sphere_case* sc, double* force3) {
+  PSL_CHECK(g && sc && force3, PSL_ERR_INVALID, "psl_sphere_force_async: null argument");
+  DeviceGuard dg(g->device);
+  const int rc = enqueue_sphere_force(g, sc, force3, cudaMemcpyDefault);
+  if (rc == 1) {  // empty box: zeros, in stream order like the non-empty case
+    PSL_CUDA(cudaMemsetAsync(g->scratch + kForceBlocks * 3, 0, 3 * sizeof(double), g->stream));
+    PSL_CUDA(cudaMemcpyAsync(force3, g->scratch + kForceBlocks * 3, 3 * sizeof(double), cudaMemcpyDefault, g->stream));
+    return PSL_OK;
+  }
+  return rc;
 }
 
 // ---- data movement ----

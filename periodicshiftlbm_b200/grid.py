@@ -341,6 +341,13 @@ def getSphereForce(grid: GridStruct, case: SphereCase) -> np.ndarray:
     return out
 
 
+def getSphereForceAsync(grid: GridStruct, case: SphereCase, out_ptr: int):
+    """Enqueue the sphere force on the grid's stream into 3 doubles at `out_ptr` (device
+    memory or pinned host memory, e.g. a pinned torch tensor's data_ptr()); valid after
+    ``grid.synchronize()``.  No host wait."""
+    call("psl_sphere_force_async", grid.handle, ctypes.byref(case.to_c()), ctypes.c_void_p(out_ptr))
+
+
 def getSphereDrag(grid: GridStruct, case: SphereCase) -> float:
     """getSphereDrag (flowAroundSphereMainSingle.cu:99-156), in lattice units of `grid`
     (before convertToPhysicalForce)."""

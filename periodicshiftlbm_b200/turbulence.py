@@ -146,6 +146,48 @@ def run(grid: GridStruct, steps: int) -> float:
     return time.perf_counter() - t
 
 
+COARSE_FORMS = (("smagorinsky_f32", "f32", False), ("smagorinsky_f16", "f16", False), ("closure_f16", "f16", True),
+                ("closure_f32", "f32", True))
+
+
+def evaluate_coarse(M: int, params: dict, u0_fine: np.ndarray, E_ref: np.ndarray, eval_steps: int, nu: float,
+                    cs: float, forms=COARSE_FORMS, say=None) -> dict:
+    """A-posteriori runs of the coarse box (M^3, every second cell of the fine start field
+    `u0_fine`) with Smagorinsky and with the closure, each after `eval_steps` steps compared
+    on the energy spectrum against `E_ref` (the box-filtered fine run)."""
+    coarse_u0 = np.ascontiguousarray(u0_fine[:, ::2, ::2, ::2])
+    kmax = M // 2
+    results = {}
+    for name, storage, closure in forms:
+        g = box_grid(M, nu, storage=storage, cs=cs)
+        if closure:
+            set_sgs_mlp(g, params, 1.0)
+        fill_from_velocity(g, coarse_u0)
+        sec = run(g, eval_steps)
+        health = g.health()
+        _, E = energy_spectrum(velocity(g))
+        results[name] = {"spectrum_error": spectrum_error(E, E_ref, kmax),
+                         "spectrum_error_k_le_32": spectrum_error(E, E_ref, min(32, kmax)),
+                         "mlups": g.cellCount * eval_steps / sec / 1e6, "health": health,
+                         "energy": float(E.sum()), "E": E.tolist()}
+        g.close()
+        if say:
+            say(f"{name}: {results[name]['spectrum_error']:.4f}")
+    return results
+
+
+def filtered_fine_spectrum(M: int, seed: int, eval_steps: int, nu: float, cs: float, k0: float = 4.0):
+    """The held-out reference: a (2M)^3 fine run (viscosity 2 nu, Smagorinsky cs) of seed
+    `seed` after 2 eval_steps steps, box-filtered 2x; returns (start field, E_ref, seconds)."""
+    fine = box_grid(2 * M, 2 * nu, cs=cs)
+    u0 = initial_velocity(2 * M, seed, k0=k0)
+    fill_from_velocity(fine, u0)
+    sec = run(fine, 2 * eval_steps)
+    _, E_ref = energy_spectrum(box_filter(velocity(fine)))
+    fine.close()
+    return u0, E_ref, sec
+
+
 def study(M: int = 256, seeds=(0, 1, 2, 3, 4, 5, 6, 7), eval_seed: int = 100, snapshots=(2000, 4000, 6000, 8000),
           eval_steps: int = 4000, nu: float = 1e-5, cs: float = 0.1, stride: int = 16, train_steps: int = 4000,
           batch: int = 65536, lr: float = 1e-3, log=None) -> dict:
@@ -193,25 +235,7 @@ def study(M: int = 256, seeds=(0, 1, 2, 3, 4, 5, 6, 7), eval_seed: int = 100, sn
     k, E_ref = energy_spectrum(box_filter(velocity(fine)))
     fine_mlups = fine.cellCount * 2 * eval_steps / fine_s / 1e6
     fine.close()
-
-    coarse_u0 = np.ascontiguousarray(u0[:, ::2, ::2, ::2])
-    kmax = M // 2
-    results = {}
-    for name, storage, closure in (("smagorinsky_f32", "f32", False), ("smagorinsky_f16", "f16", False),
-                                   ("closure_f16", "f16", True), ("closure_f32", "f32", True)):
-        g = box_grid(M, nu, storage=storage, cs=cs)
-        if closure:
-            set_sgs_mlp(g, params, 1.0)
-        fill_from_velocity(g, coarse_u0)
-        sec = run(g, eval_steps)
-        health = g.health()
-        _, E = energy_spectrum(velocity(g))
-        results[name] = {"spectrum_error": spectrum_error(E, E_ref, kmax),
-                         "spectrum_error_k_le_32": spectrum_error(E, E_ref, min(32, kmax)),
-                         "mlups": g.cellCount * eval_steps / sec / 1e6, "health": health,
-                         "energy": float(E.sum()), "E": E.tolist()}
-        g.close()
-        say(f"{name}: {results[name]['spectrum_error']:.4f}")
+    results = evaluate_coarse(M, params, u0, E_ref, eval_steps, nu, cs, say=say)
     trainer.close()
     return {"M": M, "seeds": list(seeds), "eval_seed": eval_seed, "snapshots_fine_steps": list(snapshots),
             "eval_coarse_steps": eval_steps, "nu": nu, "cs": cs, "samples": int(len(seeds) * len(snapshots) * per_snap),
@@ -237,7 +261,7 @@ def main(argv=None):
     res = study(a.M, tuple(range(a.seeds)), snapshots=tuple(int(v) for v in a.snapshots.split(",")),
                 eval_steps=a.eval_steps, stride=a.stride, train_steps=a.train_steps, batch=a.batch,
                 log=lambda *m: print(*m, file=sys.stderr, flush=True))
-    text = json.dumps(res)
+    text = json.dumps({"command": "python -m periodicshiftlbm_b200.turbulence " + " ".join(argv or sys.argv[1:]), **res})
     if a.out:
         with open(a.out, "w") as fh:
             fh.write(text)

@@ -153,3 +153,31 @@ def test_plain_kernel_on_grid_not_multiple_of_tile(orc):
     assert rel(g.populations(), o.populations()) < 1e-5
     g.close()
 
+
+
+def test_async_sphere_force_matches_synchronous():
+    """psl_sphere_force_async into pinned host memory and into device memory, several steps
+    queued before one synchronisation, equals psl_sphere_force step by step."""
+    import torch
+
+    from periodicshiftlbm_b200 import getSphereForce, getSphereForceAsync, updateGrid
+
+    cfg = config1(nx=48, ny=24, nz=24, sphere=(12.0, 12.0, 12.0), radius=4.0)
+    ga, case = make_sphere_grids(cfg)
+    gb, _ = make_sphere_grids(cfg)
+    steps = 6
+    host = torch.zeros((steps, 3), dtype=torch.float64).pin_memory()
+    dev = torch.zeros((steps, 3), dtype=torch.float64, device="cuda")
+    want = []
+    for s in range(steps):
+        updateGrid(ga, 0)
+        want.append(getSphereForce(ga[0], case))
+        updateGrid(gb, 0)
+        getSphereForceAsync(gb[0], case, host.data_ptr() + 24 * s)
+        getSphereForceAsync(gb[0], case, dev.data_ptr() + 24 * s)
+    gb[0].synchronize()
+    assert np.array_equal(host.numpy(), np.array(want))
+    assert np.array_equal(dev.cpu().numpy(), np.array(want))
+    assert np.all(np.array(want)[:, 0] != 0.0)
+    for g in ga + gb:
+        g.close()

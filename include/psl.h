@@ -88,11 +88,6 @@ int psl_grid_create(const psl_info* info, int storage, psl_grid** out);
  * periodic wrap; other grids, and grids made with PSL_GRID_ONE_MAPPING, use one plain
  * allocation.  Results are the same bits either way. */
 #define PSL_GRID_ONE_MAPPING 1u
-/* The update kernels give threads the cells of each group of 16 x-rows interior first and
- * the group's 32 x-face cells (i = 0, Nx - 1) last, in warps of their own, so that inflow /
- * outflow cells do not put the boundary branch into the fluid cells' warps (even Nx >= 4).
- * PSL_GRID_CELL_ORDER keeps plain cell order; results are the same bits either way. */
-#define PSL_GRID_CELL_ORDER 2u
 int psl_grid_create_ex(const psl_info* info, int storage, unsigned int flags, psl_grid** out);
 /* rows_mapped_twice: 1 when the rows are mapped twice; row_stride: elements from one
  * population row to the next (2N when mapped twice). */

@@ -115,16 +115,15 @@ def sponge_smagorinsky(info: InfoStruct, cs: float) -> np.ndarray:
     return np.broadcast_to(row, (nz, ny, nx)).reshape(-1).copy()
 
 
-def make_sphere_grids(cfg: SphereConfig, storage: str = "f32", one_mapping: bool = False,
-                      cell_order: bool = False) -> tuple:
+def make_sphere_grids(cfg: SphereConfig, storage: str = "f32", one_mapping: bool = False) -> tuple:
     """Allocate the grids of `cfg`, evaluate the case hooks into markers (and, for
     cs_mode 1, the coarse grid's per-cell Smagorinsky constants) and fill the start state.
-    ``one_mapping`` / ``cell_order``: the layout and thread-order options of GridStruct.
-    Returns (grids, case)."""
+    ``one_mapping``: population rows in one plain allocation (GridStruct).  Returns
+    (grids, case)."""
     case = cfg.case()
     grids = []
     for info in cfg.infos():
-        g = GridStruct(info, storage=storage, one_mapping=one_mapping, cell_order=cell_order)
+        g = GridStruct(info, storage=storage, one_mapping=one_mapping)
         setSphereCase(g, case)
         if cfg.cs_mode == 1 and info.gridID == 0:
             setSmagorinskyConstant(g, sponge_smagorinsky(info, cfg.smagorinsky))

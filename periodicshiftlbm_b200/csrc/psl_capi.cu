@@ -131,8 +131,7 @@ int psl_grid_create(const psl_info* info, int storage, psl_grid** out) {
 
 int psl_grid_create_ex(const psl_info* info, int storage, unsigned int flags, psl_grid** out) {
   PSL_CHECK(info && out, PSL_ERR_INVALID, "psl_grid_create: null argument");
-  PSL_CHECK((flags & ~(unsigned int)(PSL_GRID_ONE_MAPPING | PSL_GRID_CELL_ORDER)) == 0, PSL_ERR_INVALID,
-            "psl_grid_create: unknown flags");
+  PSL_CHECK((flags & ~(unsigned int)PSL_GRID_ONE_MAPPING) == 0, PSL_ERR_INVALID, "psl_grid_create: unknown flags");
   *out = nullptr;
   const long long nx = info->cell_count_x, ny = info->cell_count_y, nz = info->cell_count_z;
   PSL_CHECK(nx > 0 && ny > 0 && nz > 0, PSL_ERR_INVALID, "psl_grid_create: cell counts must be positive");
@@ -155,7 +154,6 @@ int psl_grid_create_ex(const psl_info* info, int storage, unsigned int flags, ps
   g->info = *info;
   g->n = (uint32_t)n;
   g->storage = storage;
-  g->cell_order = (flags & PSL_GRID_CELL_ORDER) != 0;
   g->stride = ((size_t)n + 63) / 64 * 64;
   cudaGetDevice(&g->device);
   const size_t elem = storage_bytes(storage);
@@ -498,12 +496,6 @@ int psl_apply_streaming(psl_grid* g) {
   return PSL_OK;
 }
 
-// Whether the update kernels take the cells in the grouped order (psl_rowgroups.cuh): even
-// Nx of at least 4 (whole warps of x-face cells), unless the grid asked for cell order.
-bool psl_detail_grouped_order(const psl_grid* g) {
-  return !g->cell_order && g->info.cell_count_x >= 4 && g->info.cell_count_x % 2 == 0;
-}
-
 template <typename T>
 static RelaxationT<T> relaxation(const psl_grid* g) {
   RelaxationT<T> rx;
@@ -525,20 +517,17 @@ static cudaError_t launch_step(psl_grid* g) {
   p.rx = relaxation<typename S::calc>(g);
   p.health = g->health;
   p.ri = row_index<S>(g);
-  const bool grouped = psl_detail_grouped_order(g);
-  if (grouped) p.groups = make_row_groups((uint32_t)g->info.cell_count_x, g->n / (uint32_t)g->info.cell_count_x);
   const unsigned int blocks = blocks_for(g->n, kStepThreads);
   const int addr = 27 * g->f_stride + g->n >= (1ull << 32) ? kAddrView : g->f_twice ? kAddrFlat : kAddrIndex;
   auto launch = [&](auto kernel) { kernel<<<blocks, kStepThreads, 0, g->stream>>>(p); };
-  // cell order only for odd Nx (rare; the grouped order needs whole warps of x-face cells)
   if constexpr (kCollidesOnG<S>) {
-    if (addr == kAddrView) grouped ? launch(step_kernel_g<S, kAddrView, true>) : launch(step_kernel_g<S, kAddrView, false>);
-    else if (addr == kAddrFlat) grouped ? launch(step_kernel_g<S, kAddrFlat, true>) : launch(step_kernel_g<S, kAddrFlat, false>);
-    else grouped ? launch(step_kernel_g<S, kAddrIndex, true>) : launch(step_kernel_g<S, kAddrIndex, false>);
+    if (addr == kAddrView) launch(step_kernel_g<S, kAddrView>);
+    else if (addr == kAddrFlat) launch(step_kernel_g<S, kAddrFlat>);
+    else launch(step_kernel_g<S, kAddrIndex>);
   } else {
-    if (addr == kAddrView) grouped ? launch(step_kernel<S, kAddrView, true>) : launch(step_kernel<S, kAddrView, false>);
-    else if (addr == kAddrFlat) grouped ? launch(step_kernel<S, kAddrFlat, true>) : launch(step_kernel<S, kAddrFlat, false>);
-    else grouped ? launch(step_kernel<S, kAddrIndex, true>) : launch(step_kernel<S, kAddrIndex, false>);
+    if (addr == kAddrView) launch(step_kernel<S, kAddrView>);
+    else if (addr == kAddrFlat) launch(step_kernel<S, kAddrFlat>);
+    else launch(step_kernel<S, kAddrIndex>);
   }
   return cudaGetLastError();
 }

@@ -38,7 +38,6 @@ struct psl_grid {
   bool f_twice = false; // each population row mapped twice (psl_rowmap.cu): f_stride = 2N and
                         // row element N + i is element i, so the update needs no wrap
   struct psl_row_map* f_map = nullptr;  // the mappings when f_twice, else f is one cudaMalloc
-  bool cell_order = false;  // PSL_GRID_CELL_ORDER: update threads in cell order (no x-face grouping)
   void* f = nullptr;
   uint8_t* marker = nullptr;
   float4* given = nullptr;
@@ -60,10 +59,6 @@ struct psl_grid {
   float mlp_width = 1.f;            // filter width fed to the closure
   float mlp_scalars[24] = {};       // its normalisation, b3, output scale (psl::MlpScalars)
 };
-
-// Whether the update kernels take the cells in the grouped order of psl_rowgroups.cuh
-// (psl_capi.cu): even Nx of at least 4, unless the grid was made with PSL_GRID_CELL_ORDER.
-__attribute__((visibility("hidden"))) bool psl_detail_grouped_order(const psl_grid* g);
 
 // Launches the update kernel with the learned closure (psl_learned.cu); status as psl_*.
 __attribute__((visibility("hidden"))) int psl_detail_launch_learned(psl_grid* g);

@@ -14,7 +14,6 @@
 #include "psl_collision_g.cuh"
 #include "psl_hooks.cuh"
 #include "psl_lattice.cuh"
-#include "psl_rowgroups.cuh"
 #include "psl_storage.cuh"
 
 namespace psl {
@@ -62,7 +61,6 @@ struct StepParams {
   const float* cs;       // per-cell Smagorinsky constant (getSmagorinskyConstant), or null: rx.cs18
   RelaxationT<typename S::calc> rx;
   unsigned int* health;  // bit 0 set when a collided cell's density is not finite/positive
-  RowGroups groups;      // thread-to-cell order of kGrouped launches (psl_rowgroups.cuh)
 };
 
 // The relaxation parameters of one cell: the grid's, with the cell's own Smagorinsky
@@ -314,30 +312,26 @@ __device__ __forceinline__ void update_one_cell_g(const StepParams<S>& p, uint32
 }
 
 // One thread per cell: FP32 / FP64 storage.
-// kGrouped: threads take the cells in the grouped order of psl_rowgroups.cuh (x-face cells in
-// warps of their own), else in cell order.
-template <typename S, int kAddr, bool kGrouped>
+template <typename S, int kAddr>
 __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constant__ StepParams<S> p) {
   static_assert(!kCollidesOnG<S>, "16-bit storage runs step_kernel_g");
-  const uint32_t t = blockIdx.x * kStepThreads + threadIdx.x;
-  if (t >= p.g.n) return;
-  const uint32_t cell = kGrouped ? grouped_cell(t, p.groups) : t;
+  const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
+  if (cell >= p.g.n) return;
   update_one_cell<S, kAddr>(p, cell, p.marker[cell]);
 }
 
 // One thread per cell: the 16-bit forms, held to 64 registers (8 blocks of 128 per SM;
 // 4 with 64-bit row pointers).  Left free the compiler hoists loads into 96 registers and
 // the lower occupancy costs more than the hoisting gains.
-template <typename S, int kAddr, bool kGrouped>
+template <typename S, int kAddr>
 __global__ void __launch_bounds__(kStepThreads, kAddr == kAddrView ? 4 : 8) step_kernel_g(const __grid_constant__ StepParams<S> p) {
   static_assert(kCollidesOnG<S>, "FP32 / FP64 storage runs step_kernel");
   __shared__ float slot[kStepThreads][27];
-  const uint32_t t = blockIdx.x * kStepThreads + threadIdx.x;
-  const bool in = t < p.g.n;
-  const uint32_t cell = !in ? 0u : kGrouped ? grouped_cell(t, p.groups) : t;
+  const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
+  const bool in = cell < p.g.n;
   const uint8_t m = in ? p.marker[cell] : make_marker(kSkip, 0);
   if (__all_sync(0xffffffffu, marker_kind(m) == kSkip)) return;  // ghost layers, refined interior
-  update_one_cell_g<S, kAddr>(p, cell, m, slot[threadIdx.x]);
+  update_one_cell_g<S, kAddr>(p, in ? cell : 0u, m, slot[threadIdx.x]);
 }
 
 // ------------------------------------------------------------------------------------------

@@ -125,13 +125,10 @@ int launch(psl_grid* g) {
   p.n = g->n;
   p.health = g->health;
   const unsigned int blocks = (g->n + kStepThreads - 1) / kStepThreads;
-  const bool grouped = psl_detail_grouped_order(g);
-  if (grouped) p.groups = make_row_groups((uint32_t)g->info.cell_count_x, g->n / (uint32_t)g->info.cell_count_x);
-  auto launch = [&](auto kernel) { kernel<<<blocks, kStepThreads, 0, g->stream>>>(p); };
   if (g->f_twice)
-    grouped ? launch(step_learned_warp_kernel<S, true, true>) : launch(step_learned_warp_kernel<S, true, false>);
+    step_learned_warp_kernel<S, true><<<blocks, kStepThreads, 0, g->stream>>>(p);
   else
-    grouped ? launch(step_learned_warp_kernel<S, false, true>) : launch(step_learned_warp_kernel<S, false, false>);
+    step_learned_warp_kernel<S, false><<<blocks, kStepThreads, 0, g->stream>>>(p);
   MLP_CUDA(cudaGetLastError());
   return PSL_OK;
 }

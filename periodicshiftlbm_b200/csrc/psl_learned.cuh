@@ -31,7 +31,6 @@ struct LearnedParams {
   float width;              // filter width fed to the closure (cell size / coarsest cell size)
   uint32_t n;
   unsigned int* health;
-  RowGroups groups;          // thread-to-cell order of kGrouped launches (psl_rowgroups.cuh)
 };
 
 // The closure's features from D = C - rho/3 I (the g-form moments): the same quantities
@@ -57,8 +56,7 @@ __device__ __forceinline__ void mlp_features_d(const CellMomentsG& m, float widt
 // One thread per cell with the fused closure.  16-bit storage collides on its stored
 // g = f - w (only the ten moments live across the closure's MMAs), fluid cells starting the
 // moment sums from the stored bits; FP32 runs the plain FP32 update's operation order, only
-// the rate differs.  kFlat: rows mapped twice, addressed without the wrap; kGrouped: the
-// grouped thread-to-cell order (psl_rowgroups.cuh).
+// the rate differs.  kFlat: rows mapped twice, addressed without the wrap.
 template <typename A, bool kFlat, typename S>
 __device__ __forceinline__ void load_rows(const RowIndex<S>& r, uint32_t cell, typename A::calc (&f)[27]) {
   if constexpr (kFlat) load_cell_flat<A>(r, cell, f);
@@ -70,16 +68,14 @@ __device__ __forceinline__ void store_rows(const RowIndex<S>& r, uint32_t cell, 
   else store_cell_as<A>(r, cell, f);
 }
 
-template <typename S, bool kFlat, bool kGrouped>
+template <typename S, bool kFlat>
 __global__ void __launch_bounds__(kStepThreads, 6) step_learned_warp_kernel(const __grid_constant__ LearnedParams<S> p) {
   __shared__ __align__(16) float bc_slot[kStepThreads][27];
   // the warp's FP16 feature tile lives in its own lanes' boundary slots (free after the
   // __syncwarp that follows every lane's boundary condition)
   __half* xt = reinterpret_cast<__half*>(&bc_slot[threadIdx.x & ~31u][0]);
-  const uint32_t t = blockIdx.x * kStepThreads + threadIdx.x;
-  const bool in = t < p.n;
-  const uint32_t cell = !in ? 0u : kGrouped ? grouped_cell(t, p.groups) : t;
-  const uint8_t m = in ? p.marker[cell] : make_marker(kSkip, 0);
+  const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
+  const uint8_t m = cell < p.n ? p.marker[cell] : make_marker(kSkip, 0);
   const int kind = marker_kind(m);
   float x[kMlpIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   float f[27];

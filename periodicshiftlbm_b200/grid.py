@@ -114,17 +114,14 @@ class GridStruct:
     """One PS grid on the GPU (GridStruct, include/types.h:77): metadata, the [27][N]
     population array and the 27 periodic shifts.  Owns its device memory."""
 
-    def __init__(self, Info: InfoStruct, storage: str = "f32", one_mapping: bool = False, cell_order: bool = False):
+    def __init__(self, Info: InfoStruct, storage: str = "f32", one_mapping: bool = False):
         """``one_mapping``: keep the population rows in one plain allocation even where they
-        could be mapped twice; ``cell_order``: update threads in plain cell order instead of
-        the grouped order with x-face warps (psl.h, psl_grid_create_ex).  Either way the
-        results are the same bits."""
+        could be mapped twice (psl.h, psl_grid_create_ex); the results are the same bits."""
         self.Info = Info
         self.storage = storage
         self._h = ctypes.c_void_p()
-        flags = (1 if one_mapping else 0) | (2 if cell_order else 0)
-        call("psl_grid_create_ex", ctypes.byref(Info.to_c()), _lib.STORAGE[storage], ctypes.c_uint(flags),
-             ctypes.byref(self._h))
+        call("psl_grid_create_ex", ctypes.byref(Info.to_c()), _lib.STORAGE[storage],
+             ctypes.c_uint(1 if one_mapping else 0), ctypes.byref(self._h))
 
     @property
     def rows_mapped_twice(self) -> bool:

@@ -1,11 +1,9 @@
-"""Population rows mapped twice in virtual memory (psl_rowmap.cu) and the grouped
-thread-to-cell order of the update kernels (psl_rowgroups.cuh).
+"""Population rows mapped twice in virtual memory (psl_rowmap.cu).
 
 A grid whose row size is a whole number of the driver's mapping granularity maps every
 population row twice back to back, and the update kernels then read cell + shift without
-the periodic wrap; grids of even Nx give the x-face cells warps of their own.  Neither
-changes any arithmetic, so grids made with PSL_GRID_ONE_MAPPING and / or
-PSL_GRID_CELL_ORDER must give the same bits after any number of steps: the plain and the
+the periodic wrap.  Everything else about the grid is unchanged, so a grid made with
+PSL_GRID_ONE_MAPPING must give the same bits after any number of steps: the plain and the
 closure update, every storage form, arbitrary shifts (wrap points anywhere in the rows),
 a refined two-level run whose fine grid keeps one mapping.
 """
@@ -52,11 +50,11 @@ def _random_shifts(n, seed):
 
 @pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
 @pytest.mark.parametrize("closure", [False, True])
-def test_layouts_and_thread_orders_give_the_same_bits(storage, closure):
+def test_twice_mapped_equals_one_mapping(storage, closure):
     cfg = config2(scale=0.5)          # coarse 256x128x128: rows of 8 / 16 MiB, mapped twice
     runs = []
-    for one, cell_order in ((False, False), (True, False), (True, True)):
-        grids, case = make_sphere_grids(cfg, storage=storage, one_mapping=one, cell_order=cell_order)
+    for one in (False, True):
+        grids, case = make_sphere_grids(cfg, storage=storage, one_mapping=one)
         assert grids[0].rows_mapped_twice == (not one)
         assert not grids[1].rows_mapped_twice  # 128x96x96 fine cells: not a whole number of 2 MiB
         sh = _random_shifts(grids[0].cellCount, 5)
@@ -72,13 +70,11 @@ def test_layouts_and_thread_orders_give_the_same_bits(storage, closure):
             updateGrid(grids, 0)
             drags.append(getSphereDrag(grids[1], case))
         runs.append((grids, [g.fArray for g in grids], [g.shifter for g in grids], drags))
-    ga, fa, sa, da = runs[0]
-    for gb, fb, sb, db in runs[1:]:
-        for lvl in range(2):
-            assert np.array_equal(sa[lvl], sb[lvl])
-            assert np.array_equal(fa[lvl], fb[lvl]), (lvl, np.abs(fa[lvl] - fb[lvl]).max())
-        assert da == db
-    for grids, *_ in runs:
-        for g in grids:
-            assert g.health() == 0
-            g.close()
+    (ga, fa, sa, da), (gb, fb, sb, db) = runs
+    for lvl in range(2):
+        assert np.array_equal(sa[lvl], sb[lvl])
+        assert np.array_equal(fa[lvl], fb[lvl]), (lvl, np.abs(fa[lvl] - fb[lvl]).max())
+    assert da == db
+    for g in ga + gb:
+        assert g.health() == 0
+        g.close()

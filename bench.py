@@ -69,6 +69,13 @@ def workload(args):
     return config2(scale=args.scale) if args.config == 2 else config1()
 
 
+def full_size_name() -> str:
+    """The workload the committed ncu traffic figures were captured on (config 2, scale 1)."""
+    from periodicshiftlbm_b200.cases import config2
+
+    return config2().name
+
+
 def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
@@ -174,7 +181,9 @@ def hbm_peak():
 
 def update_kernel(storage: str, sgs: str) -> str:
     """The coarse-grid update kernel the library launches for this form."""
-    return "step_learned_warp_kernel" if sgs == "mlp" else "step_kernel"
+    if sgs == "mlp":
+        return "step_learned_warp_kernel"
+    return "step_kernel_g" if storage in ("f16", "bf16") else "step_kernel"
 
 
 def batch_traffic(storage: str, cells: int):
@@ -289,7 +298,8 @@ def measure_form(args, cfg, storage: str, sgs: str, world: int, local: int, with
     out["roofline"] = {
         "bound": "hbm", "kernel": kernel + " (coarse grid)", "achieved": round(achieved, 1), "peak": peak,
         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-        "traffic": ncu_traffic(kernel, storage), "algorithmic_bytes_per_launch": bpu * coarse_updates,
+        "traffic": ncu_traffic(kernel, storage) if cfg.name == full_size_name() else None,
+        "algorithmic_bytes_per_launch": bpu * coarse_updates,
         "launch_ms": round(out["coarse_ms"], 4),
         "fine_launch_ms": round(out["fine_ms"], 4) if out["fine_ms"] else None,
         "whole_step_frac": round(bpu * updates / (ms / args.steps * 1e-3) / 1e9 / peak, 4),

@@ -240,8 +240,9 @@ int psl_export_section_cut(psl_grid* grid, int plane, int cut, float rho_nominal
  * Work is queued on cuda_stream (NULL = legacy default stream); nothing is synchronised.
  * Partial sums live in a fixed 24.6 KB array inside the library, held by every GPU that
  * loads it until exit; the box may hold at most 4,194,304 cells (else PSL_ERR_INVALID).
- * The first call on a device looks that array up (cudaGetSymbolAddress) with the device
- * current: make it before any stream capture.  All calls share the array, so calls whose
+ * Calls outside stream capture look that array up (cudaGetSymbolAddress, current device);
+ * calls inside capture reuse the last address found outside it, so make one call outside
+ * capture first (after a device reset too).  All calls share the array, so calls whose
  * kernels overlap on the GPU (different streams) race; order them on one stream. */
 int psl_momentum_exchange_force_noalloc(const float* populations, long long row_stride, const int* shifts27,
                                         long long cell_count, const uint8_t* markers, int nx, int ny, int nz,

@@ -32,8 +32,8 @@ constexpr int kMaxDevices = 64;
 // 1024 x 3 partials + 3 spare doubles: 24.6 KB per device.
 static __device__ __align__(256) double psl_noalloc_force_scratch[kNoAllocBlocks * 3 + 3];
 
-// Device address of the scratch array, looked up once per device.  In host code the
-// array's name is only a host-side stand-in, never a device address.
+// Device address of the scratch array per device (scratch_on_current_device).  In host code
+// the array's name is only a host-side stand-in, never a device address.
 double* g_scratch[kMaxDevices] = {};
 std::mutex g_scratch_mutex;
 
@@ -49,17 +49,30 @@ int noalloc_fail(int code, const std::string& msg) {
   return code;
 }
 
-int scratch_on_current_device(double** out) {
+// The scratch array's device address on the current device.  Outside stream capture it is
+// looked up on every call (a device reset reloads the module, and a cached address would go
+// stale); during capture, where a lookup could load the module inside the capture, the
+// address of the last call outside capture is used.
+int scratch_on_current_device(cudaStream_t stream, double** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return noalloc_fail(PSL_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(PSL_ERR_CUDA, "device ordinal out of range");
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &capture) != cudaSuccess) {
+    cudaGetLastError();
+    capture = cudaStreamCaptureStatusActive;  // status unknown: do not touch the module
+  }
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch[dev]) {
+  if (capture == cudaStreamCaptureStatusNone || !g_scratch[dev]) {
     double* p = nullptr;
     e = cudaGetSymbolAddress((void**)&p, psl_noalloc_force_scratch);
     if (e != cudaSuccess || !p)
-      return noalloc_fail(PSL_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      return noalloc_fail(PSL_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e) +
+                                            (capture == cudaStreamCaptureStatusNone
+                                                 ? ""
+                                                 : " (first call inside stream capture: make one call outside "
+                                                   "capture first)"));
     g_scratch[dev] = p;
   }
   *out = g_scratch[dev];
@@ -91,10 +104,10 @@ int psl_momentum_exchange_force_noalloc(const float* populations, long long row_
     return noalloc_fail(PSL_ERR_INVALID,
                         "psl_momentum_exchange_force_noalloc: box has " + std::to_string(cells) +
                             " cells, more than the fixed scratch serves (" + std::to_string(kNoAllocMaxBoxCells) + ")");
-  double* scratch = nullptr;
-  const int rc = scratch_on_current_device(&scratch);
-  if (rc != PSL_OK) return rc;
   cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  double* scratch = nullptr;
+  const int rc = scratch_on_current_device(stream, &scratch);
+  if (rc != PSL_OK) return rc;
   GridView<StoreF32> g;
   for (int q = 0; q < 27; ++q) {
     g.fq[q] = const_cast<float*>(populations) + (size_t)q * (size_t)row_stride;

@@ -99,3 +99,60 @@ def test_noalloc_force_rejects_boxes_beyond_its_fixed_scratch():
         lo.ctypes.data, hi.ctypes.data, ctypes.c_void_p(out.data_ptr()), None)
     assert rc == 1
     assert b"4194304" in L.psl_last_error()
+
+
+def test_noalloc_force_in_a_captured_graph_and_after_a_larger_box():
+    """One call outside capture, then a call captured into a CUDA graph (stream capture
+    fails on any allocation or synchronisation) and replayed; and a call over the whole grid
+    before the sphere's box, so the fixed partial sums hold more blocks than the second call
+    writes.  Both give psl_sphere_force's result."""
+    import torch
+
+    from periodicshiftlbm_b200 import _lib, getSphereForce, updateGrid
+    from periodicshiftlbm_b200.cases import SphereConfig, make_sphere_grids
+
+    cfg = SphereConfig(name="noalloc", nx=48, ny=24, nz=24, sphere=(14.0, 12.0, 12.0), radius=4.0, u_in=0.05,
+                       nu=0.01, smagorinsky=0.1)
+    grids, case = make_sphere_grids(cfg)
+    g = grids[0]
+    info = g.Info
+    n = info.cellCount
+    for _ in range(9):
+        updateGrid(grids, 0)
+    want = getSphereForce(g, case)
+    lo, hi = _box(case, info)
+    whole_lo = np.zeros(3, dtype=np.int32)
+    whole_hi = np.array([info.cellCountX, info.cellCountY, info.cellCountZ], dtype=np.int32)
+    L = _lib.lib()
+    shifts = g.shifter.astype(np.int32)
+    rows = torch.from_numpy(_rows_with_shifts(g.fArray, shifts, n)).cuda()
+    markers = torch.from_numpy(g.markers).cuda()
+    out = torch.full((3,), float("nan"), dtype=torch.float64, device="cuda")
+    whole = torch.full((3,), float("nan"), dtype=torch.float64, device="cuda")
+    s = torch.cuda.Stream()
+
+    def call(box_lo, box_hi, dst):
+        return L.psl_momentum_exchange_force_noalloc(
+            ctypes.c_void_p(rows.data_ptr()), n, shifts.ctypes.data, n, ctypes.c_void_p(markers.data_ptr()),
+            info.cellCountX, info.cellCountY, info.cellCountZ, box_lo.ctypes.data, box_hi.ctypes.data,
+            ctypes.c_void_p(dst.data_ptr()), ctypes.c_void_p(s.cuda_stream))
+
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        assert call(whole_lo, whole_hi, whole) == 0, L.psl_last_error()  # outside capture, larger box
+        assert call(lo, hi, out) == 0, L.psl_last_error()                # then the sphere's box
+    torch.cuda.synchronize()
+    assert np.allclose(out.cpu().numpy(), want, rtol=TOL, atol=TOL * np.abs(want).max())
+    out.fill_(float("nan"))
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s):
+        assert call(lo, hi, out) == 0, L.psl_last_error()
+    torch.cuda.synchronize()
+    graph.replay()
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    assert np.allclose(got, want, rtol=TOL, atol=TOL * np.abs(want).max()), (got, want)
+    assert np.all(np.isfinite(whole.cpu().numpy()))
+    del graph
+    for gr in grids:
+        gr.close()

@@ -6,11 +6,15 @@
 //   g++ -O2 -std=c++17 -I include examples/flow_around_sphere.cpp
 //       periodicshiftlbm_b200/libpsl_b200.so -Wl,-rpath,$PWD/periodicshiftlbm_b200 -o sphere
 //   (one command line)
-//   ./sphere [steps] [scale]
+//   ./sphere [steps] [scale] [sponge]
+// With "sponge" the coarse grid takes a per-cell getSmagorinskyConstant hook: C_s rising
+// linearly from the case's constant at i = 3 Nx / 4 to four times it at the outlet
+// (periodicshiftlbm_b200.cases.sponge_smagorinsky is the same hook in Python).
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "psl.hpp"
@@ -18,6 +22,7 @@
 int main(int argc, char** argv) {
   const int steps = argc > 1 ? std::atoi(argv[1]) : 100;
   const double scale = argc > 2 ? std::atof(argv[2]) : 1.0;
+  const bool sponge = argc > 3 && std::string(argv[3]) == "sponge";
   auto sc_len = [&](double v) { return (int)std::lround(v * scale); };
   psl_sphere_case sc{};
   sc.sphere_x = sc.sphere_y = sc.sphere_z = (float)(128.0 * scale);
@@ -53,6 +58,15 @@ int main(int argc, char** argv) {
   for (auto& g : grids) {
     psl::setSphereCase(g, sc);
     psl::fillEquilibriumFromFunction(g, sc);
+  }
+  if (sponge) {
+    const float cs = sc.smagorinsky;
+    psl::setSmagorinskyConstant(grids[0], [cs](int i, int, int, const psl::InfoStruct& I) {
+      const int i0 = (3 * I.cellCountX) / 4;
+      float ramp = 3.f * (float)(i - i0);
+      ramp = ramp / (float)(I.cellCountX - 1 - i0);
+      return i > i0 ? cs * (1.f + ramp) : cs;
+    });
   }
   const auto t0 = std::chrono::steady_clock::now();
   double drag = 0.0;

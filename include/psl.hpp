@@ -134,7 +134,23 @@ inline void fillEquilibriumUniform(GridStruct& g, float rho, float ux, float uy,
 inline void setSphereCase(GridStruct& g, const psl_sphere_case& sc) {
   check(psl_apply_sphere_case(g.handle(), &sc), "setSphereCase");
 }
-// updateGrid recursion of the case driver (flowAroundSphereMainSingle.cu:158-167).
+// A case's getSmagorinskyConstant(i, j, k, Info) hook (include/applyLocalCellUpdate.h:68),
+// any callable with that signature returning the constant: evaluated once per cell on the
+// host, in cell order, and kept on the device as the grid's per-cell field.
+template <typename Hook>
+inline void setSmagorinskyConstant(GridStruct& g, Hook&& getSmagorinskyConstant) {
+  const InfoStruct& I = g.Info;
+  std::vector<float> cs((size_t)I.cellCountX * I.cellCountY * I.cellCountZ);
+  size_t c = 0;
+  for (int k = 0; k < I.cellCountZ; ++k)
+    for (int j = 0; j < I.cellCountY; ++j)
+      for (int i = 0; i < I.cellCountX; ++i) cs[c++] = (float)getSmagorinskyConstant(i, j, k, I);
+  check(psl_set_smagorinsky_field(g.handle(), cs.data()), "setSmagorinskyConstant");
+}
+// The uniform form (one constant for every cell; 0 disables LES).
+inline void setSmagorinskyConstant(GridStruct& g, float cs) {
+  check(psl_set_smagorinsky(g.handle(), cs), "setSmagorinskyConstant");
+}
 // The customised update (moving walls, forced-velocity cells, body force): see
 // psl_set_body_force in psl.h for the marker bytes.
 inline void setBodyForce(GridStruct& g, float gx, float gy, float gz) {
@@ -145,6 +161,7 @@ inline void getTorque(GridStruct& g, const int lo[3], const int hi[3], const flo
   check(psl_torque(g.handle(), lo, hi, point, torque, force), "getTorque");
 }
 
+// updateGrid recursion of the case driver (flowAroundSphereMainSingle.cu:158-167).
 inline void updateGrid(std::vector<GridStruct>& grids, int level) {
   std::vector<psl_grid*> h(grids.size());
   for (size_t i = 0; i < grids.size(); ++i) h[i] = grids[i].handle();
@@ -156,5 +173,11 @@ inline double getSphereDrag(GridStruct& g, const psl_sphere_case& sc) {
   check(psl_sphere_force(g.handle(), &sc, f), "getSphereDrag");
   return f[0];
 }
+// The same force queued without a host wait: `force3` (device or pinned host memory) holds
+// it once the grid's stream has passed this call (synchronize()).
+inline void getSphereForceAsync(GridStruct& g, const psl_sphere_case& sc, double* force3) {
+  check(psl_sphere_force_async(g.handle(), &sc, force3), "getSphereForceAsync");
+}
+inline void synchronize(GridStruct& g) { check(psl_synchronize(g.handle()), "synchronize"); }
 
 }  // namespace psl

@@ -37,14 +37,18 @@ def test_mirror_and_example_compile_and_link():
 
 
 @pytest.mark.gpu
-def test_example_drag_equals_python_api():
+@pytest.mark.parametrize("sponge", [False, True])
+def test_example_drag_equals_python_api(sponge):
+    """Also with the C++ per-cell getSmagorinskyConstant hook against the same hook in
+    Python (cases.sponge_smagorinsky, SphereConfig.cs_mode = 1)."""
     from periodicshiftlbm_b200 import getSphereDrag, updateGrid
     from periodicshiftlbm_b200.cases import config2, make_sphere_grids
 
     scale, steps = 0.125, 12
-    out = subprocess.run([build_example(), str(steps), str(scale)], check=True, capture_output=True, text=True).stdout
+    cmd = [build_example(), str(steps), str(scale)] + (["sponge"] if sponge else [])
+    out = subprocess.run(cmd, check=True, capture_output=True, text=True).stdout
     drag_cpp = float(re.search(r"drag (\S+)", out).group(1))
-    grids, case = make_sphere_grids(config2(scale=scale))
+    grids, case = make_sphere_grids(config2(scale=scale, cs_mode=1 if sponge else 0))
     for _ in range(steps):
         updateGrid(grids, 0)
     drag_py = getSphereDrag(grids[1], case)

@@ -267,8 +267,8 @@ __device__ __forceinline__ void update_one_cell(const StepParams<S>& p, uint32_t
 // 21-72): solid cells swap the bits; fluid cells start the moment sums from them
 // (raw_moments_g_bits); boundary cells go through f = g + w for the boundary functions; all
 // collide on g (psl_collision_g.cuh), bitwise as collide_cell_g on the converted values.
-// `slot`: the thread's shared-memory slot for the boundary functions.  Written for the
-// register allocator: the collided cells' loads and stores are predicated on one flag
+// `slot`: the thread's shared-memory slot for the boundary functions.  All 32 lanes of the
+// warp call it together (the boundary test is warp-wide).  Written for the register allocator: the collided cells' loads and stores are predicated on one flag
 // instead of sitting behind early returns (which cost ~50 spilled registers at the 64-register
 // cap), and lanes that do not collide run the arithmetic on zeros.  `cell` must be < N.
 template <typename S, int kAddr>
@@ -295,14 +295,21 @@ __device__ __forceinline__ void update_one_cell_g(const StepParams<S>& p, uint32
   }
   float g[27];
   CellMomentsG cm;
-  if (!collides || kind == kFluid) {
+  const bool bc = collides && kind != kFluid;
+  if (!__any_sync(0xffffffffu, bc)) {
     cm = cell_moments_from_raw(raw_moments_g_bits<S::kind == kStoreBF16>(h));
   } else {
+    // a warp holding boundary cells sums every lane's moments from converted values (the
+    // same bits as from the stored bits), so its fluid lanes do not run a second sum
 #pragma unroll
-    for (int q = 0; q < 27; ++q) g[q] = B::to_float(h[q]) + lattice_weight(q);
-    apply_boundary_at(m, g, p.given ? p.given[cell] : p.given_uniform, slot);
+    for (int q = 0; q < 27; ++q) g[q] = B::to_float(h[q]);
+    if (bc) {
 #pragma unroll
-    for (int q = 0; q < 27; ++q) g[q] -= lattice_weight(q);
+      for (int q = 0; q < 27; ++q) g[q] += lattice_weight(q);
+      apply_boundary_at(m, g, p.given ? p.given[cell] : p.given_uniform, slot);
+#pragma unroll
+      for (int q = 0; q < 27; ++q) g[q] -= lattice_weight(q);
+    }
     cm = cell_moments_g(g);
   }
   if (collides && p.health && !finite_density(cm.rho)) atomicOr(p.health, 1u);

@@ -34,7 +34,9 @@ struct LearnedParams {
 };
 
 // The closure's features from D = C - rho/3 I (the g-form moments): the same quantities
-// as mlp_features (Pi_neq = D / rho, its trace, norm and det / |Pi|^2, the filter width).
+// as mlp_features (Pi_neq = D / rho, its trace, norm and det / |Pi|^2, the filter width),
+// with the single-instruction square root and reciprocal of the g-form collision (the
+// features enter the network as FP16).
 __device__ __forceinline__ void mlp_features_d(const CellMomentsG& m, float width, float (&x)[kMlpIn]) {
   const float r = m.inv_rho;
   const float pxx = m.dxx * r, pyy = m.dyy * r, pzz = m.dzz * r;
@@ -48,8 +50,8 @@ __device__ __forceinline__ void mlp_features_d(const CellMomentsG& m, float widt
   x[4] = pxz;
   x[5] = pyz;
   x[6] = pxx + pyy + pzz;
-  x[7] = sqrtf(n2);
-  x[8] = det / (n2 + 1e-30f);
+  x[7] = gsqrt(n2);
+  x[8] = det * grecip(n2 + 1e-30f);
   x[9] = width;
 }
 
@@ -95,24 +97,31 @@ __global__ void __launch_bounds__(kStepThreads, 6) step_learned_warp_kernel(cons
     }
     if (collides) load_rows<B, kFlat>(p.ri, cell, h);
     CellMomentsG cm{};
-    if (collides) {
-      if (kind == kFluid) {
-        cm = cell_moments_from_raw(raw_moments_g_bits<S::kind == kStoreBF16>(h));
-      } else {
+    const bool bc = collides && kind != kFluid;
+    if (!__any_sync(0xffffffffu, bc)) {
+      if (collides) cm = cell_moments_from_raw(raw_moments_g_bits<S::kind == kStoreBF16>(h));
+    } else if (collides) {
+      // a warp holding boundary cells sums every lane's moments from converted values (the
+      // same bits as from the stored bits)
 #pragma unroll
-        for (int q = 0; q < 27; ++q) f[q] = B::to_float(h[q]) + lattice_weight(q);
+      for (int q = 0; q < 27; ++q) f[q] = B::to_float(h[q]);
+      if (bc) {
+#pragma unroll
+        for (int q = 0; q < 27; ++q) f[q] += lattice_weight(q);
         apply_boundary_at(m, f, p.given ? p.given[cell] : p.given_uniform, bc_slot[threadIdx.x]);
 #pragma unroll
         for (int q = 0; q < 27; ++q) f[q] -= lattice_weight(q);
-        cm = cell_moments_g(f);
       }
+      cm = cell_moments_g(f);
+    }
+    if (collides) {
       if (p.health && !finite_density(cm.rho)) atomicOr(p.health, 1u);
       mlp_features_d(cm, p.width, x);
     }
     __syncwarp();
     const float nu_t = mlp_warp_eval(p.mlpw, p.sc, xt, x);
     if (collides) {
-      relax_rebuild_g(f, cm, 1.f / (3.f * (p.nu + nu_t) + 0.5f));
+      relax_rebuild_g(f, cm, grecip(3.f * (p.nu + nu_t) + 0.5f));
       store_rows<StoredOf<S>, kFlat>(p.ri, cell, f);
     }
   } else {

@@ -651,7 +651,8 @@ static int launch_coarse_fine(psl_grid* c, psl_grid* f) {
   if (p.kE < p.cnz - 1) p.face_active |= 32;
   const long long ra = a - 2, rb = b - 2, rc = cc - 2;
   p.n_ring = (uint32_t)(ra * rb * rc - (ra - 2) * (rb - 2) * (rc - 2));
-  p.n_shell = (uint32_t)((long long)p.fnx * p.fny * p.fnz - (long long)(p.fnx - 4) * (p.fny - 4) * (p.fnz - 4));
+  // z faces, y faces, then four lanes per x-row boundary (coarse_fine_kernel)
+  p.n_shell = (uint32_t)(4LL * p.fnx * p.fny + 4LL * p.fnx * (p.fnz - 4) + 4LL * (p.fny - 3) * (p.fnz - 4));
   p.barrier = c->health + 1;
   p.error = c->health;
   int sms = 0, per_sm = 0;

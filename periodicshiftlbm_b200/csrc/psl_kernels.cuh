@@ -807,13 +807,16 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
       k = 2 + r / nx;
       i = r % nx;
     } else {
-      // x faces: lanes 2m and 2m+1 take the two cells of one row (i and i+1, the same coarse
-      // parent), so each store covers 8 contiguous bytes instead of 4 bytes of a line
-      const uint32_t u = t - zl - yl, per_side = 2u * (ny - 4) * (nz - 4);
-      const uint32_t side = u / per_side, w = u % per_side, r = w >> 1;
-      i = (side ? nx - 2 : 0) + (int)(w & 1u);
-      j = 2 + r % (ny - 4);
-      k = 2 + r / (ny - 4);
+      // x faces: four lanes per row boundary take the end of row j - 1 (i = Nx - 2, Nx - 1)
+      // and the start of row j (i = 0, 1), four consecutive cells in memory, so each
+      // population's store covers 16 contiguous bytes; at j = 2 and j = Ny - 2 one side of
+      // the boundary is a y-face row (its cells are y-face items) and those lanes idle
+      const uint32_t u = t - zl - yl, per_k = 4u * (ny - 3);
+      const uint32_t b = (u % per_k) >> 2, sub = u & 3u;
+      k = 2 + (int)(u / per_k);
+      j = 2 + (int)b - (sub < 2 ? 1 : 0);
+      i = sub < 2 ? nx - 2 + (int)sub : (int)sub - 2;
+      if (j < 2 || j >= ny - 2) continue;
     }
     const uint32_t fcell = ((uint32_t)k * ny + j) * nx + i;
     const uint8_t fm = p.fine_marker[fcell];

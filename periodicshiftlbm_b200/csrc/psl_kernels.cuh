@@ -780,8 +780,10 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
         rk = 1 + r / a;
         ri = r % a;
       } else {
-        const uint32_t u = t - faceK - faceJ, layer = u / ((b - 2) * (c - 2)), r = u % ((b - 2) * (c - 2));
-        ri = layer ? a - 1 : 0;
+        // x faces: neighbouring lanes take the start- and end-face ring cells of one (j, k), so
+        // a warp reads both ends of the same fine rows, whose child pairs share sectors
+        const uint32_t u = t - faceK - faceJ, r = u >> 1;
+        ri = (u & 1u) ? a - 1 : 0;
         rj = 1 + r % (b - 2);
         rk = 1 + r / (b - 2);
       }

@@ -18,6 +18,20 @@ namespace psl {
 
 enum StorageKind : int { kStoreF32 = 0, kStoreF16 = 1, kStoreBF16 = 2, kStoreF64 = 3 };
 
+// Read-only loads of the update kernels with a 256-byte L2 prefetch hint: a warp reads 64
+// (16-bit) or 128 (FP32) contiguous bytes of a row, and the warps of the next cells read
+// the rest of the same lines.
+__device__ __forceinline__ float ldg_row(const float* p) {
+  float v;
+  asm("ld.global.nc.L2::256B.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ uint16_t ldg_row(const uint16_t* p) {
+  uint16_t v;
+  asm("ld.global.nc.L2::256B.b16 %0, [%1];" : "=h"(v) : "l"(p));
+  return v;
+}
+
 struct StoreF32 {
   using type = float;
   using calc = float;
@@ -31,7 +45,7 @@ struct StoreF32 {
   // Update-kernel forms: each element is read once by its owning cell (read-only path)
   // and then overwritten by it (evict-first store).
   template <int Q>
-  __device__ __forceinline__ static float load_once(const float* p) { return __ldg(p); }
+  __device__ __forceinline__ static float load_once(const float* p) { return ldg_row(p); }
   template <int Q>
   __device__ __forceinline__ static void store_once(float* p, float v) { __stcs(p, v); }
 };
@@ -140,7 +154,7 @@ struct StoredBits {
   using calc = uint16_t;
   template <int Q>
   __device__ __forceinline__ static uint16_t load_once(const type* p) {
-    return __ldg(reinterpret_cast<const unsigned short*>(p));
+    return ldg_row(reinterpret_cast<const uint16_t*>(p));
   }
   template <int Q>
   __device__ __forceinline__ static void store_once(type* p, uint16_t v) {

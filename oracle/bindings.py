@@ -175,6 +175,17 @@ class Sim:
         """The reference's getTorque written for PS grids (reference build only)."""
         return float(self.owner.lib.ref_sim_torque(self.h, level))
 
+    def flow_report(self, level: int, plane: str, cut_index: int, bounds6) -> dict:
+        """The reference's getFlowReportGeneral over this level alone, as a one-level DIAD
+        grid holding the level's state (reference build only)."""
+        planes = {"XY": 0, "ZY": 1, "ZX": 2}
+        b = np.ascontiguousarray(bounds6, dtype=np.float32)
+        out = np.zeros(5, dtype=np.float32)
+        self.owner.lib.ref_sim_flow_report_single(self.h, level, planes[plane], cut_index, b.ctypes.data,
+                                                  out.ctypes.data)
+        return {"ux": float(out[0]), "uy": float(out[1]), "uz": float(out[2]), "rho": float(out[3]),
+                "area": float(out[4])}
+
     def export_section(self, level: int, plane: str, cut_index: int, plot_number: int, path: str):
         """The reference's exportSectionCutPlotGeneral of one level, written to `path`
         (reference build only)."""
@@ -215,6 +226,7 @@ class RefLib(_SimLib):
         L.ref_sim_export_section.argtypes = [vp, i, i, i, i, ctypes.c_char_p]
         L.ref_sim_torque.argtypes = [vp, i]
         L.ref_sim_torque.restype = f
+        L.ref_sim_flow_report_single.argtypes = [vp, i, i, i, vp, vp]
         L.ref_export_history.argtypes = [vp, i, i, ctypes.c_char_p]
         for n in ("ref_sim_periodic_x", "ref_sim_periodic_y", "ref_sim_streaming"):
             getattr(L, n).argtypes = [vp, i]

@@ -195,6 +195,7 @@ static FILE* ref_export_fopen(const char* path, const char* mode) {
 using std::max;
 #define fopen ref_export_fopen
 #include "include/plotter/exportSectionCutPlot.h"
+#include "include/flowReportFunctions.h"
 #undef fopen
 
 // getForcing (the hook of M35Full/m35Main.cu:101-119) of the forced-velocity annulus:
@@ -366,12 +367,64 @@ static void updateLevel(RefSim& sim, int level) {
 
 extern "C" {
 
+void ref_sim_get_f(void* h, int level, float* out);
+
 // exportSectionCutPlotGeneral (exportSectionCutPlot.h:2-89) of one level, written to `path`.
 void ref_sim_export_section(void* p, int level, int plane, int cutIndex, int plotNumber, const char* path) {
   RefSim* sim = static_cast<RefSim*>(p);
   g_export_path = path;
   exportSectionCutPlotGeneral(sim->grids[level], cutIndex, plotNumber, static_cast<PlaneEnum>(plane));
   g_export_path = nullptr;
+}
+
+// getFlowReportGeneral (flowReportFunctions.h:2-251) of one level, run by the reference's own
+// code on a one-level DIAD grid that holds the level's state: the IJK arrays list every cell
+// in cell order, every Esotwist neighbour of a cell is the cell itself, so the read index of
+// direction q is (fIndex[q], cell), and the populations are placed there (the PS layout has
+// no DIAD counterpart across levels -- its fine grids are offset by half a fine cell -- so
+// only single levels compare).  out5 = (ux, uy, uz, rho, area mm^2).
+void ref_sim_flow_report_single(void* p, int level, int plane, int cutIndex, const float* bounds6, float* out5) {
+  GridStruct& g = static_cast<RefSim*>(p)->grids[level];
+  const int N = g.Info.cellCount;
+  std::vector<float> f((size_t)27 * N);
+  ref_sim_get_f(p, level, f.data());
+  DIADGridStruct d;
+  d.Info = g.Info;
+  d.Info.gridID = 0;  // the only level of the report
+  d.esotwistFlipper = false;
+  d.fArray.setSizes(27, N);
+  d.IJK.iArray.setSize(N);
+  d.IJK.jArray.setSize(N);
+  d.IJK.kArray.setSize(N);
+  IntArrayType* nbr[7] = {&d.EsotwistNbrArray.iNbrArray, &d.EsotwistNbrArray.jNbrArray, &d.EsotwistNbrArray.kNbrArray,
+                          &d.EsotwistNbrArray.ijNbrArray, &d.EsotwistNbrArray.ikNbrArray,
+                          &d.EsotwistNbrArray.jkNbrArray, &d.EsotwistNbrArray.ijkNbrArray};
+  for (IntArrayType* a : nbr) a->setSize(N);
+  auto fv = d.fArray.getView();
+  auto iv = d.IJK.iArray.getView();
+  auto jv = d.IJK.jArray.getView();
+  auto kv = d.IJK.kArray.getView();
+  const int nx = g.Info.cellCountX, ny = g.Info.cellCountY;
+  for (int c = 0; c < N; ++c) {
+    iv[c] = c % nx;
+    jv[c] = (c / nx) % ny;
+    kv[c] = c / (nx * ny);
+    for (IntArrayType* a : nbr) a->getView()[c] = c;
+    DIADEsotwistNbrStruct self{c, c, c, c, c, c, c};
+    int cellIndex[27], fIndex[27];
+    getEsotwistWriteIndex(c, cellIndex, fIndex, self, d.esotwistFlipper, d.Info);
+    for (int q = 0; q < 27; ++q) fv(fIndex[q], cellIndex[q]) = f[(size_t)q * N + c];
+  }
+  std::vector<DIADGridStruct> grids(1);
+  grids[0] = std::move(d);
+  XYZBoundsStruct b{bounds6[0], bounds6[1], bounds6[2], bounds6[3], bounds6[4], bounds6[5]};
+  FlowReportStruct r;
+  getFlowReportGeneral(grids, cutIndex, b, r, static_cast<PlaneEnum>(plane));
+  out5[0] = r.ux;
+  out5[1] = r.uy;
+  out5[2] = r.uz;
+  out5[3] = r.rho;
+  out5[4] = r.areamm2;
 }
 
 // getTorque of one level (forced-velocity annulus of the case).

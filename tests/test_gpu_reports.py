@@ -83,3 +83,28 @@ def test_flow_report_two_levels_uses_the_fine_grid_inside_the_block():
     assert rep["area"] == pytest.approx(keep.sum() * 0.25)
     assert rep["ux"] == pytest.approx((j[0] / rho)[cut][keep].mean(), rel=1e-6)
     s.close()
+
+
+@pytest.mark.parametrize("plane,cut,bounds", [("XY", 9, (-1, -1, -1, 100, 100, 100)),
+                                              ("ZY", 12, (-1, -1, -1, 100, 100, 100)),
+                                              ("ZX", 7, (-1, -1, -1, 100, 100, 100)),
+                                              ("XY", 8, (6.5, 3.2, -1, 21.7, 14.1, 100)),
+                                              ("ZY", 15, (-1, 2.5, 4.0, 100, 15.5, 12.2))])
+def test_flow_report_matches_the_reference_function(ref, plane, cut, bounds):
+    """psl_get_flow_report of one level against the reference's own getFlowReportGeneral
+    (flowReportFunctions.h:2-251) compiled for the host, run on a one-level DIAD grid that
+    holds the same state (the PS grid's populations after 20 steps); the reference sums in
+    FP32, this library in FP64."""
+    c = SphereCase(nx=28, ny=18, nz=16, sphere=(12.0, 9.0, 8.0), radius=4.0, nu=0.01)
+    s = GpuSim(c)
+    s.run(20)
+    g = s.grids[0]
+    r = ref.sim(c)
+    r.set_populations(g.fArray, 0)
+    want = r.flow_report(0, plane, cut, bounds)
+    got = getFlowReport([g], plane, cut, bounds)
+    assert got["area"] == want["area"] and want["area"] > 0
+    for name in ("ux", "uy", "uz", "rho"):
+        assert got[name] == pytest.approx(want[name], rel=2e-5, abs=1e-7), (name, got[name], want[name])
+    r.close()
+    s.close()

@@ -805,8 +805,35 @@ int psl_sphere_force_async(psl_grid* g, const psl_sphere_case* sc, double* force
 }
 
 // ---- data movement ----
+// FP32 storage needs no conversion: logical row q is the stored row rotated by shift_q
+// (cell c at (c + shift_q) mod N), so it moves with plain copies -- one contiguous range on
+// twice-mapped rows (the second mapping holds the wrap), else the two pieces of the
+// rotation -- without a staging buffer or a kernel.
+static cudaError_t copy_rows_f32(psl_grid* g, float* host, bool to_host) {
+  float* base = static_cast<float*>(g->f);
+  const size_t n = g->n;
+  for (int q = 0; q < 27; ++q) {
+    float* row = base + (size_t)q * g->f_stride;
+    float* h = host + (size_t)q * n;
+    const size_t sh = g->shift[q];
+    const size_t first = g->f_twice ? n : n - sh;  // elements of the first piece
+    cudaError_t e = to_host ? cudaMemcpyAsync(h, row + sh, first * sizeof(float), cudaMemcpyDeviceToHost, g->stream)
+                            : cudaMemcpyAsync(row + sh, h, first * sizeof(float), cudaMemcpyHostToDevice, g->stream);
+    if (e == cudaSuccess && first < n)
+      e = to_host ? cudaMemcpyAsync(h + first, row, (n - first) * sizeof(float), cudaMemcpyDeviceToHost, g->stream)
+                  : cudaMemcpyAsync(row, h + first, (n - first) * sizeof(float), cudaMemcpyHostToDevice, g->stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaStreamSynchronize(g->stream);
+}
+
 template <typename S>
 static int gather(psl_grid* g, float* host) {
+  if constexpr (S::kind == kStoreF32) {
+    const cudaError_t e = copy_rows_f32(g, host, true);
+    if (e != cudaSuccess) return fail(PSL_ERR_CUDA, std::string("psl_get_populations: ") + cudaGetErrorString(e));
+    return PSL_OK;
+  }
   float* tmp = nullptr;
   PSL_CUDA(cudaMalloc(&tmp, (size_t)g->n * sizeof(float)));
   cudaError_t e = cudaSuccess;
@@ -826,6 +853,11 @@ static int gather(psl_grid* g, float* host) {
 
 template <typename S>
 static int scatter(psl_grid* g, const float* host) {
+  if constexpr (S::kind == kStoreF32) {
+    const cudaError_t e = copy_rows_f32(g, const_cast<float*>(host), false);
+    if (e != cudaSuccess) return fail(PSL_ERR_CUDA, std::string("psl_set_populations: ") + cudaGetErrorString(e));
+    return PSL_OK;
+  }
   float* tmp = nullptr;
   PSL_CUDA(cudaMalloc(&tmp, (size_t)g->n * sizeof(float)));
   cudaError_t e = cudaSuccess;

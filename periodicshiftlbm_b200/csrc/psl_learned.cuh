@@ -70,8 +70,10 @@ __device__ __forceinline__ void store_rows(const RowIndex<S>& r, uint32_t cell, 
   else store_cell_as<A>(r, cell, f);
 }
 
+// 7 blocks of 128 per SM (72 registers; ptxas keeps ~40 bytes in local memory, L1-resident):
+// 1.2% faster than 6 blocks at 80 registers without spills, measured on the sphere case.
 template <typename S, bool kFlat>
-__global__ void __launch_bounds__(kStepThreads, 6) step_learned_warp_kernel(const __grid_constant__ LearnedParams<S> p) {
+__global__ void __launch_bounds__(kStepThreads, 7) step_learned_warp_kernel(const __grid_constant__ LearnedParams<S> p) {
   __shared__ __align__(16) float bc_slot[kStepThreads][27];
   // the warp's FP16 feature tile lives in its own lanes' boundary slots (free after the
   // __syncwarp that follows every lane's boundary condition)

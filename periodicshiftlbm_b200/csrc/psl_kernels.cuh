@@ -711,21 +711,20 @@ __device__ __forceinline__ void restrict_cell(const RowIndex<S>& rc, const RowIn
                                               int i, int j, int k) {
   using T = typename S::calc;
   const int fi = (i - p.iS) * 2, fj = (j - p.jS) * 2, fk = (k - p.kS) * 2;
+  uint32_t fc[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c)
+    fc[c] = ((uint32_t)(fk + (c >> 2)) * p.fny + (fj + ((c >> 1) & 1))) * p.fnx + (fi + (c & 1));
+  // population by population (the eight children of one population are independent loads),
+  // each summed in the child order
   T f[27];
 #pragma unroll
-  for (int q = 0; q < 27; ++q) f[q] = T(0);
+  for (int q = 0; q < 27; ++q) {
+    T v = T(0);
 #pragma unroll
-  for (int dk = 0; dk <= 1; ++dk)
-#pragma unroll
-    for (int dj = 0; dj <= 1; ++dj)
-#pragma unroll
-      for (int di = 0; di <= 1; ++di) {
-        const uint32_t fc = ((uint32_t)(fk + dk) * p.fny + (fj + dj)) * p.fnx + (fi + di);
-#pragma unroll
-        for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], load_pop(rf, q, fc));
-      }
-#pragma unroll
-  for (int q = 0; q < 27; ++q) f[q] = f[q] * T(0.125);
+    for (int c = 0; c < 8; ++c) v = rn_add(v, load_pop(rf, q, fc[c]));
+    f[q] = v * T(0.125);
+  }
   rescale(f, false);
   const uint32_t cc = ((uint32_t)k * p.cny + j) * p.cnx + i;
 #pragma unroll
@@ -836,12 +835,11 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
     if (!mask) continue;
     const int ic = i / 2 + p.iS, jc = j / 2 + p.jS, kc = k / 2 + p.kS;
     const T d[3] = {T((i & 1) ? 0.25f : -0.25f), T((j & 1) ? 0.25f : -0.25f), T((k & 1) ? 0.25f : -0.25f)};
-    T f[27];
     const uint32_t pc = ((uint32_t)kc * p.cny + jc) * p.cnx + ic;
-#pragma unroll
-    for (int q = 0; q < 27; ++q) f[q] = load_pop(rc, q, pc);
     const int cidx[3] = {ic, jc, kc};
     const int cdim[3] = {p.cnx, p.cny, p.cnz};
+    uint32_t nc[6];  // the six neighbours in the order (x+, x-, y+, y-, z+, z-)
+    T w[6];
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
       int plus = cidx[ax] + 1, minus = cidx[ax] - 1;
@@ -852,11 +850,18 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
       for (int side = 0; side < 2; ++side) {
         int nb[3] = {ic, jc, kc};
         nb[ax] = side == 0 ? plus : minus;
-        const T w = (side == 0 ? inv : -inv) * d[ax];  // exact: powers of two
-        const uint32_t nc = ((uint32_t)nb[2] * p.cny + nb[1]) * p.cnx + nb[0];
-#pragma unroll
-        for (int q = 0; q < 27; ++q) f[q] = rn_add(f[q], load_pop(rc, q, nc) * w);
+        w[2 * ax + side] = (side == 0 ? inv : -inv) * d[ax];  // exact: powers of two
+        nc[2 * ax + side] = ((uint32_t)nb[2] * p.cny + nb[1]) * p.cnx + nb[0];
       }
+    }
+    // population by population, the parent first and then the six neighbours in that order
+    T f[27];
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+      T v = load_pop(rc, q, pc);
+#pragma unroll
+      for (int t = 0; t < 6; ++t) v = rn_add(v, load_pop(rc, q, nc[t]) * w[t]);
+      f[q] = v;
     }
     rescale(f, true);
 #pragma unroll

@@ -60,6 +60,19 @@ def test_null_grid_arguments_rejected():
     assert L.psl_apply_local_cell_update(None) == 1
     assert L.psl_apply_streaming(None) == 1
     assert L.psl_apply_coarse_fine_grid_communication(None, None) == 1
+    assert L.psl_sphere_force_async(None, None, None) == 1
+    assert L.psl_grid_get_layout(None, None, None) == 1
+
+
+def test_unknown_grid_flags_rejected():
+    """psl_grid_create_ex accepts PSL_GRID_ONE_MAPPING (1) only; anything else is refused
+    before any device work."""
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    for flags in (2, 4, 0x80000000):
+        assert L.psl_grid_create_ex(ctypes.byref(_info(8, 8, 8)), 0, flags, ctypes.byref(h)) == 1
+        assert b"flags" in L.psl_last_error()
+        assert not h.value
 
 
 def _has_gpu():

@@ -268,9 +268,10 @@ __device__ __forceinline__ void update_one_cell(const StepParams<S>& p, uint32_t
 // (raw_moments_g_bits); boundary cells go through f = g + w for the boundary functions; all
 // collide on g (psl_collision_g.cuh), bitwise as collide_cell_g on the converted values.
 // `slot`: the thread's shared-memory slot for the boundary functions.  All 32 lanes of the
-// warp call it together (the boundary test is warp-wide).  Written for the register allocator: the collided cells' loads and stores are predicated on one flag
-// instead of sitting behind early returns (which cost ~50 spilled registers at the 64-register
-// cap), and lanes that do not collide run the arithmetic on zeros.  `cell` must be < N.
+// warp call it together (the boundary test is warp-wide).  Written for the register
+// allocator: the loads and the collision run on every lane and only the stores are
+// predicated, instead of early returns (which cost ~50 spilled registers at the 64-register
+// cap).  `cell` must be < N.
 template <typename S, int kAddr>
 __device__ __forceinline__ void update_one_cell_g(const StepParams<S>& p, uint32_t cell, uint8_t m, float* slot) {
   using B = StoredBits<S>;
@@ -286,13 +287,11 @@ __device__ __forceinline__ void update_one_cell_g(const StepParams<S>& p, uint32
     }
     store_for<B, kAddr>(p, cell, h);
   }
+  // every lane loads (a lane that does not collide -- a skipped cell in a mixed warp, a lane
+  // past the grid on cell 0 -- computes on real values and stores nothing): cheaper than
+  // predicating the loads and zeroing the rest
+  load_for<B, kAddr>(p, cell, h);
   const bool collides = kind != kSkip && kind != kSolid;
-  if (collides) {
-    load_for<B, kAddr>(p, cell, h);
-  } else {
-#pragma unroll
-    for (int q = 0; q < 27; ++q) h[q] = 0;
-  }
   float g[27];
   CellMomentsG cm;
   const bool bc = collides && kind != kFluid;

@@ -496,6 +496,13 @@ int psl_apply_streaming(psl_grid* g) {
   return PSL_OK;
 }
 
+// Thread-to-cell rotation of the update kernels (cell_of_thread): half a warp when the x-rows
+// are whole warps long, so that each row boundary's two x-face cells share one warp.
+uint32_t psl_detail_thread_rotation(const psl_grid* g) {
+  return (g->info.cell_count_x % 32 == 0 && g->n > 16) ? 16u : 0u;
+}
+static uint32_t thread_rotation(const psl_grid* g) { return psl_detail_thread_rotation(g); }
+
 template <typename T>
 static RelaxationT<T> relaxation(const psl_grid* g) {
   RelaxationT<T> rx;
@@ -517,6 +524,7 @@ static cudaError_t launch_step(psl_grid* g) {
   p.rx = relaxation<typename S::calc>(g);
   p.health = g->health;
   p.ri = row_index<S>(g);
+  p.rot = thread_rotation(g);
   const unsigned int blocks = blocks_for(g->n, kStepThreads);
   const int addr = 27 * g->f_stride + g->n >= (1ull << 32) ? kAddrView : g->f_twice ? kAddrFlat : kAddrIndex;
   auto launch = [&](auto kernel) { kernel<<<blocks, kStepThreads, 0, g->stream>>>(p); };

@@ -60,6 +60,10 @@ struct psl_grid {
   float mlp_scalars[24] = {};       // its normalisation, b3, output scale (psl::MlpScalars)
 };
 
+// Thread-to-cell rotation of the update kernels (psl_capi.cu, cell_of_thread in
+// psl_kernels.cuh).
+__attribute__((visibility("hidden"))) uint32_t psl_detail_thread_rotation(const psl_grid* g);
+
 // Launches the update kernel with the learned closure (psl_learned.cu); status as psl_*.
 __attribute__((visibility("hidden"))) int psl_detail_launch_learned(psl_grid* g);
 

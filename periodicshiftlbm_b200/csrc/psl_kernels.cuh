@@ -61,7 +61,16 @@ struct StepParams {
   const float* cs;       // per-cell Smagorinsky constant (getSmagorinskyConstant), or null: rx.cs18
   RelaxationT<typename S::calc> rx;
   unsigned int* health;  // bit 0 set when a collided cell's density is not finite/positive
+  uint32_t rot;          // thread-to-cell rotation (cell_of_thread)
 };
+
+// Cell of thread t: t - rot, cyclically.  With rot = 16 and Nx a multiple of 32, the last
+// cell of one x-row and the first of the next (both x-face cells, i = Nx - 1 and i = 0) fall
+// into the same warp, so only one warp in Nx / 32 carries the boundary branch instead of two
+// (every cell still updated once; the warps still cover 32 consecutive cells).
+__device__ __forceinline__ uint32_t cell_of_thread(uint32_t t, uint32_t rot, uint32_t n) {
+  return t >= rot ? t - rot : t + n - rot;
+}
 
 // The relaxation parameters of one cell: the grid's, with the cell's own Smagorinsky
 // constant when the grid has a per-cell field.
@@ -321,8 +330,9 @@ __device__ __forceinline__ void update_one_cell_g(const StepParams<S>& p, uint32
 template <typename S, int kAddr>
 __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constant__ StepParams<S> p) {
   static_assert(!kCollidesOnG<S>, "16-bit storage runs step_kernel_g");
-  const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
-  if (cell >= p.g.n) return;
+  const uint32_t t = blockIdx.x * kStepThreads + threadIdx.x;
+  if (t >= p.g.n) return;
+  const uint32_t cell = cell_of_thread(t, p.rot, p.g.n);
   update_one_cell<S, kAddr>(p, cell, p.marker[cell]);
 }
 
@@ -333,11 +343,12 @@ template <typename S, int kAddr>
 __global__ void __launch_bounds__(kStepThreads, kAddr == kAddrView ? 4 : 8) step_kernel_g(const __grid_constant__ StepParams<S> p) {
   static_assert(kCollidesOnG<S>, "FP32 / FP64 storage runs step_kernel");
   __shared__ float slot[kStepThreads][27];
-  const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
-  const bool in = cell < p.g.n;
+  const uint32_t t = blockIdx.x * kStepThreads + threadIdx.x;
+  const bool in = t < p.g.n;
+  const uint32_t cell = in ? cell_of_thread(t, p.rot, p.g.n) : 0u;
   const uint8_t m = in ? p.marker[cell] : make_marker(kSkip, 0);
   if (__all_sync(0xffffffffu, marker_kind(m) == kSkip)) return;  // ghost layers, refined interior
-  update_one_cell_g<S, kAddr>(p, in ? cell : 0u, m, slot[threadIdx.x]);
+  update_one_cell_g<S, kAddr>(p, cell, m, slot[threadIdx.x]);
 }
 
 // ------------------------------------------------------------------------------------------

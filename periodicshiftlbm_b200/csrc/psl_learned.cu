@@ -124,6 +124,7 @@ int launch(psl_grid* g) {
   p.width = g->mlp_width;
   p.n = g->n;
   p.health = g->health;
+  p.rot = psl_detail_thread_rotation(g);
   const unsigned int blocks = (g->n + kStepThreads - 1) / kStepThreads;
   if (g->f_twice)
     step_learned_warp_kernel<S, true><<<blocks, kStepThreads, 0, g->stream>>>(p);

@@ -31,6 +31,7 @@ struct LearnedParams {
   float width;              // filter width fed to the closure (cell size / coarsest cell size)
   uint32_t n;
   unsigned int* health;
+  uint32_t rot;              // thread-to-cell rotation (cell_of_thread)
 };
 
 // The closure's features from D = C - rho/3 I (the g-form moments): the same quantities
@@ -78,8 +79,10 @@ __global__ void __launch_bounds__(kStepThreads, 7) step_learned_warp_kernel(cons
   // the warp's FP16 feature tile lives in its own lanes' boundary slots (free after the
   // __syncwarp that follows every lane's boundary condition)
   __half* xt = reinterpret_cast<__half*>(&bc_slot[threadIdx.x & ~31u][0]);
-  const uint32_t cell = blockIdx.x * kStepThreads + threadIdx.x;
-  const uint8_t m = cell < p.n ? p.marker[cell] : make_marker(kSkip, 0);
+  const uint32_t t = blockIdx.x * kStepThreads + threadIdx.x;
+  const bool in = t < p.n;
+  const uint32_t cell = in ? cell_of_thread(t, p.rot, p.n) : 0u;
+  const uint8_t m = in ? p.marker[cell] : make_marker(kSkip, 0);
   const int kind = marker_kind(m);
   float x[kMlpIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   float f[27];

@@ -529,9 +529,10 @@ static cudaError_t launch_step(psl_grid* g) {
   const int addr = 27 * g->f_stride + g->n >= (1ull << 32) ? kAddrView : g->f_twice ? kAddrFlat : kAddrIndex;
   auto launch = [&](auto kernel) { kernel<<<blocks, kStepThreads, 0, g->stream>>>(p); };
   if constexpr (kCollidesOnG<S>) {
-    if (addr == kAddrView) launch(step_kernel_g<S, kAddrView>);
-    else if (addr == kAddrFlat) launch(step_kernel_g<S, kAddrFlat>);
-    else launch(step_kernel_g<S, kAddrIndex>);
+    const bool cs = g->cs_field != nullptr;
+    if (addr == kAddrView) cs ? launch(step_kernel_g<S, kAddrView, true>) : launch(step_kernel_g<S, kAddrView, false>);
+    else if (addr == kAddrFlat) cs ? launch(step_kernel_g<S, kAddrFlat, true>) : launch(step_kernel_g<S, kAddrFlat, false>);
+    else cs ? launch(step_kernel_g<S, kAddrIndex, true>) : launch(step_kernel_g<S, kAddrIndex, false>);
   } else {
     if (addr == kAddrView) launch(step_kernel<S, kAddrView>);
     else if (addr == kAddrFlat) launch(step_kernel<S, kAddrFlat>);

@@ -281,7 +281,7 @@ __device__ __forceinline__ void update_one_cell(const StepParams<S>& p, uint32_t
 // allocator: the loads and the collision run on every lane and only the stores are
 // predicated, instead of early returns (which cost ~50 spilled registers at the 64-register
 // cap).  `cell` must be < N.
-template <typename S, int kAddr>
+template <typename S, int kAddr, bool kCsField>
 __device__ __forceinline__ void update_one_cell_g(const StepParams<S>& p, uint32_t cell, uint8_t m, float* slot) {
   using B = StoredBits<S>;
   const int kind = marker_kind(m);
@@ -321,7 +321,7 @@ __device__ __forceinline__ void update_one_cell_g(const StepParams<S>& p, uint32
     cm = cell_moments_g(g);
   }
   if (collides && p.health && !finite_density(cm.rho)) atomicOr(p.health, 1u);
-  const float cs18 = collides && p.cs ? 18.f * p.cs[cell] : p.rx.cs18;
+  const float cs18 = kCsField && collides ? 18.f * p.cs[cell] : p.rx.cs18;
   relax_rebuild_g(g, cm, smagorinsky_omega_g(cm, p.rx.omega0, p.rx.tau, p.rx.tau2, cs18));
   if (collides) store_for<StoredOf<S>, kAddr>(p, cell, g);
 }
@@ -339,7 +339,8 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constan
 // One thread per cell: the 16-bit forms, held to 64 registers (8 blocks of 128 per SM;
 // 4 with 64-bit row pointers).  Left free the compiler hoists loads into 96 registers and
 // the lower occupancy costs more than the hoisting gains.
-template <typename S, int kAddr>
+// kCsField: the grid has a per-cell Smagorinsky field (p.cs), else the uniform constant.
+template <typename S, int kAddr, bool kCsField>
 __global__ void __launch_bounds__(kStepThreads, kAddr == kAddrView ? 4 : 8) step_kernel_g(const __grid_constant__ StepParams<S> p) {
   static_assert(kCollidesOnG<S>, "FP32 / FP64 storage runs step_kernel");
   __shared__ float slot[kStepThreads][27];
@@ -348,7 +349,7 @@ __global__ void __launch_bounds__(kStepThreads, kAddr == kAddrView ? 4 : 8) step
   const uint32_t cell = in ? cell_of_thread(t, p.rot, p.g.n) : 0u;
   const uint8_t m = in ? p.marker[cell] : make_marker(kSkip, 0);
   if (__all_sync(0xffffffffu, marker_kind(m) == kSkip)) return;  // ghost layers, refined interior
-  update_one_cell_g<S, kAddr>(p, cell, m, slot[threadIdx.x]);
+  update_one_cell_g<S, kAddr, kCsField>(p, cell, m, slot[threadIdx.x]);
 }
 
 // ------------------------------------------------------------------------------------------

@@ -21,9 +21,10 @@ state is uploaded from pinned host memory, every step's FP64 drag is copied back
 host memory in stream order (the reference driver reads it every step), the final state is
 downloaded, and the run synchronises once at the end.  The default FP32 plain
 run also measures the metric's second form on the same case and step counts --
-`forms.f16_mlp`: FP16 f - w storage with the learned closure -- with its roofline, its
-speed-up over the plain form and its long-run drag error against the plain form (from the
-committed precision record; `--no-forms` skips it).
+`forms.f16_mlp`: FP16 f - w storage with the learned closure, its network run on every
+`--sgs-interval`-th update (default 4) and each cell's kept nu_t in between -- with its
+roofline, its speed-up over the plain form and its long-run drag error against the plain
+form (from the committed precision record; `--no-forms` skips it).
 """
 from __future__ import annotations
 
@@ -58,6 +59,9 @@ def parse():
     p.add_argument("--form", default="single", choices=["single", "batch"])
     p.add_argument("--sgs", default="smagorinsky", choices=["smagorinsky", "mlp"],
                    help="mlp: the learned closure trained on decaying turbulence (packaged weights)")
+    p.add_argument("--sgs-interval", type=int, default=4,
+                   help="the learned closure's network on every K-th update, the kept nu_t in between "
+                        "(16-bit storage; psl_set_sgs_mlp_interval; 1: every update)")
     p.add_argument("--batch-cases", type=int, default=64)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-steps", type=int, default=2)
@@ -189,6 +193,12 @@ def update_kernel(storage: str, sgs: str) -> str:
     return "step_kernel_g" if storage in ("f16", "bf16") else "step_kernel"
 
 
+def closure_interval(storage: str, sgs: str, interval: int) -> int:
+    """Updates per run of the closure's network (1 unless a 16-bit form runs it on every
+    interval-th update)."""
+    return interval if sgs == "mlp" and storage in ("f16", "bf16") and interval > 1 else 1
+
+
 def batch_traffic(storage: str, cells: int):
     """DRAM bytes per launch of the batched update: the per-cell traffic of the committed
     16-case capture (profiles/batch_step_kernel_batch16.md, FP32) times the cells."""
@@ -199,13 +209,15 @@ def batch_traffic(storage: str, cells: int):
     return round(float(m.group(1)) * cells) if m else None
 
 
-def long_run_drag_error():
+def long_run_drag_error(interval: int = 1):
     """|C_d(FP16 + closure) / C_d(plain FP32) - 1| of the long-run means in the committed
-    precision record (python -m periodicshiftlbm_b200.precision, 40,000 steps), or None."""
+    precision record (python -m periodicshiftlbm_b200.precision, 100,000 steps) for the
+    closure run on every `interval`-th update, or None."""
     path = os.path.join(REPO, "periodicshiftlbm_b200", "data", "study_precision_sphere256.json")
     try:
         forms = json.load(open(path))["forms"]
-        return round(abs(forms["f16+mlp"]["cd_mean"] / forms["f32"]["cd_mean"] - 1.0), 5)
+        key = "f16+mlp" if interval <= 1 else f"f16+mlp{interval}"
+        return round(abs(forms[key]["cd_mean"] / forms["f32"]["cd_mean"] - 1.0), 5)
     except (OSError, KeyError, ValueError):
         return None
 
@@ -247,7 +259,8 @@ def measure_form(args, cfg, storage: str, sgs: str, world: int, local: int, with
 
         closure = load_params()
         for g in grids:
-            set_sgs_mlp(g, closure, g.Info.res / grids[0].Info.res)
+            set_sgs_mlp(g, closure, g.Info.res / grids[0].Info.res,
+                        interval=args.sgs_interval if storage in ("f16", "bf16") else None)
     torch.cuda.synchronize()
     levels = len(grids)
     ev = {"coarse": [], "fine": []}
@@ -305,14 +318,26 @@ def measure_form(args, cfg, storage: str, sgs: str, world: int, local: int, with
     if cfg.refine:
         (i0, j0, k0), (i1, j1, k1) = cfg.refine
         coarse_updates -= (i1 - i0 - 4) * (j1 - j0 - 4) * (k1 - k0 - 4)
-    bpu = BYTES_PER_UPDATE[storage]
+    every = closure_interval(storage, sgs, args.sgs_interval)
+    # with a closure interval each update also moves the cell's kept nu_t (2 bytes): written
+    # by the closure's run, read by the updates between
+    bpu = BYTES_PER_UPDATE[storage] + (2 if every > 1 else 0)
     peak, peak_kind = hbm_peak()
     achieved = bpu * coarse_updates / (out["coarse_ms"] * 1e-3) / 1e9
     kernel = update_kernel(storage, sgs)
+    label = kernel + " (coarse grid)"
+    traffic = ncu_traffic(kernel, storage) if cfg.name == full_size_name() else None
+    if every > 1:
+        label = (f"{kernel} on every {every}th update, step_kernel_g with the kept nu_t between "
+                 "(coarse grid, mean launch)")
+        held = ncu_traffic("step_kernel_g_nu", storage) if cfg.name == full_size_name() else None
+        # the network's run was captured at interval 1: add the nu_t it stores (2 bytes a cell)
+        traffic = (round((traffic + 2 * coarse_updates + (every - 1) * held) / every)
+                   if traffic and held else None)
     out["roofline"] = {
-        "bound": "hbm", "kernel": kernel + " (coarse grid)", "achieved": round(achieved, 1), "peak": peak,
+        "bound": "hbm", "kernel": label, "achieved": round(achieved, 1), "peak": peak,
         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-        "traffic": ncu_traffic(kernel, storage) if cfg.name == full_size_name() else None,
+        "traffic": traffic,
         "algorithmic_bytes_per_launch": bpu * coarse_updates,
         "launch_ms": round(out["coarse_ms"], 4),
         "fine_launch_ms": round(out["fine_ms"], 4) if out["fine_ms"] else None,
@@ -383,7 +408,7 @@ def run_native(args):
         "vs_baseline": None,
         "dtype": "f32" if args.storage == "f32" else f"{args.storage}-storage/f32-math",
         "data": "synthetic",
-        "config": config_dict(cfg, args.storage, args.sgs, world),
+        "config": config_dict(cfg, args.storage, args.sgs, world, args.sgs_interval),
         "roofline": main["roofline"],
         "e2e": main["e2e"],
         "gpu_launches": args.steps * (1 + 3 * (levels - 1)),
@@ -403,13 +428,15 @@ def run_native(args):
                           "drag_after_timed": plain_drag},
             "f16_mlp": {"value": round(alt["value"], 1), "ms_per_step": round(alt["ms"] / args.steps, 4),
                         "speedup_vs_f32_plain": round(alt["value"] / main["value"], 3),
+                        "closure_interval": args.sgs_interval,
                         "roofline": alt["roofline"], "clocks": alt["clocks"],
                         "drag_after_timed": alt["drag_after_timed"],
-                        "drag_rel_vs_f32_plain": long_run_drag_error(),
+                        "drag_rel_vs_f32_plain": long_run_drag_error(args.sgs_interval),
                         "drag_rel_vs_f32_plain_after_timed": round(
                             abs(alt["drag_after_timed"] - plain_drag) / abs(plain_drag), 5),
-                        "note": "drag_rel_vs_f32_plain: mean drag coefficient over steps 20,001-40,000 of the "
-                                "half-scale case, FP16 + closure against plain FP32, from the committed "
+                        "note": "drag_rel_vs_f32_plain: mean drag coefficient over steps 20,001-100,000 of the "
+                                "half-scale case, FP16 + closure (the same interval) against plain FP32, "
+                                "from the committed "
                                 "precision record (periodicshiftlbm_b200/data/study_precision_sphere256.json); "
                                 "..._after_timed: instantaneous drag after this run's warm-up + timed steps "
                                 "from the same start, inside the start-up transient"},
@@ -424,8 +451,9 @@ def run_native(args):
         print(json.dumps(line), flush=True)
 
 
-def config_dict(cfg, storage: str, sgs: str, world: int) -> dict:
+def config_dict(cfg, storage: str, sgs: str, world: int, interval: int = 1) -> dict:
     """The `config` of a bench line; the reference arm reports the same keys."""
+    every = "" if interval <= 1 or storage == "f32" else f", network on every {interval}th update, kept nu_t between"
     return {
         "workload": cfg.name,
         "grid": [cfg.nx, cfg.ny, cfg.nz],
@@ -433,7 +461,7 @@ def config_dict(cfg, storage: str, sgs: str, world: int) -> dict:
         "storage": storage,
         "updates_per_step": cfg.updates_per_step(),
         "reference_formula_updates_per_step": cfg.reference_updates_per_step(),
-        "collision": ("cumulant + learned MLP closure (per-warp tensor-core MMAs)" if sgs == "mlp" else
+        "collision": (f"cumulant + learned MLP closure (per-warp tensor-core MMAs{every})" if sgs == "mlp" else
                       "cumulant + Smagorinsky" if cfg.smagorinsky else "cumulant"),
         "l2": "inputs larger than L2 (no flush)" if cfg.refine else "state fits partly in L2",
         "parallelism": f"replicas x{world}",

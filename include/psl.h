@@ -272,6 +272,14 @@ typedef struct psl_sgs_mlp {
  * grid's).  Cells fall back to Smagorinsky if the closure's tensor-core step times out
  * (health bit 2). */
 int psl_set_sgs_mlp(psl_grid* grid, const psl_sgs_mlp* mlp, float filter_width);
+/* Run the closure on every `interval`-th psl_apply_local_cell_update of `grid` only (1, the
+ * default: every update).  That update keeps each collided cell's nu_t as FP16 (2 bytes per
+ * cell on the device); the updates in between relax with the kept nu_t and skip the
+ * network.  16-bit storage (FP16 / BF16) only.  The first update after this call, after
+ * psl_set_sgs_mlp, and after populations, markers or shifts are set from outside the update
+ * (fill, set, case, fillCoarseGridFromFine) always runs the closure.  No reference
+ * counterpart. */
+int psl_set_sgs_mlp_interval(psl_grid* grid, int interval);
 /* The closure alone on host features (count x 10 raw features) -> nu_t (count floats),
  * through the same tensor-core device code (parity tests). */
 int psl_sgs_mlp_infer(const psl_sgs_mlp* mlp, const float* features, int count, float* nu_t);

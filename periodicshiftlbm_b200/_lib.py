@@ -116,6 +116,7 @@ _SIGNATURES = {
     "psl_get_populations": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_get_macroscopic": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_set_sgs_mlp": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PslSgsMlp), ctypes.c_float]),
+    "psl_set_sgs_mlp_interval": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "psl_sgs_mlp_infer": (ctypes.c_int, [ctypes.POINTER(PslSgsMlp), ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "psl_fill_equilibrium_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "psl_sgs_trainer_create": (ctypes.c_int, [ctypes.c_longlong, ctypes.POINTER(ctypes.c_void_p)]),

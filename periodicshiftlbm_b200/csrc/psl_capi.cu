@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "psl.h"
@@ -201,6 +202,7 @@ int psl_grid_destroy(psl_grid* g) {
   if (g->T) cudaFree(g->T);
   if (g->givenT) cudaFree(g->givenT);
   if (g->cs_field) cudaFree(g->cs_field);
+  if (g->mlp_nut) cudaFree(g->mlp_nut);
   delete g;
   return PSL_OK;
 }
@@ -229,6 +231,7 @@ int psl_grid_get_info(const psl_grid* g, psl_info* info, long long* cell_count, 
 // ---- hooks ----
 int psl_apply_sphere_case(psl_grid* g, const psl_sphere_case* sc) {
   PSL_CHECK(g && sc, PSL_ERR_INVALID, "psl_apply_sphere_case: null argument");
+  psl_detail_closure_stale(g);
   DeviceGuard dg(g->device);
   fill_markers_kernel<SphereCase><<<blocks_for(g->n, 256), 256, 0, g->stream>>>(sphere_hooks(sc), hook_info(g), g->n,
                                                                                  g->marker, nullptr);
@@ -240,6 +243,7 @@ int psl_apply_sphere_case(psl_grid* g, const psl_sphere_case* sc) {
 
 int psl_set_markers(psl_grid* g, const uint8_t* host) {
   PSL_CHECK(g && host, PSL_ERR_INVALID, "psl_set_markers: null argument");
+  psl_detail_closure_stale(g);
   DeviceGuard dg(g->device);
   // moving walls (solid, normal bits 1) and forced-velocity cells (fluid, normal bits 1)
   // select the customised update kernel
@@ -450,17 +454,20 @@ static int fill_eq(psl_grid* g, const Case& c) {
 
 int psl_fill_equilibrium_sphere(psl_grid* g, const psl_sphere_case* sc) {
   PSL_CHECK(g && sc, PSL_ERR_INVALID, "psl_fill_equilibrium_sphere: null argument");
+  psl_detail_closure_stale(g);
   return fill_eq(g, sphere_hooks(sc));
 }
 
 int psl_fill_equilibrium_uniform(psl_grid* g, float rho, float ux, float uy, float uz) {
   PSL_CHECK(g, PSL_ERR_INVALID, "psl_fill_equilibrium_uniform: null grid");
+  psl_detail_closure_stale(g);
   UniformCase c{rho, ux, uy, uz};
   return fill_eq(g, c);
 }
 
 int psl_fill_equilibrium_field(psl_grid* g, const float* rho_u) {
   PSL_CHECK(g && rho_u, PSL_ERR_INVALID, "psl_fill_equilibrium_field: null argument");
+  psl_detail_closure_stale(g);
   DeviceGuard dg(g->device);
   float* tmp = nullptr;
   PSL_CUDA(cudaMalloc(&tmp, (size_t)g->n * 4 * sizeof(float)));
@@ -513,8 +520,9 @@ static RelaxationT<T> relaxation(const psl_grid* g) {
   return rx;
 }
 
+// held_nu: the update between two evaluations of the learned closure, on its held nu_t.
 template <typename S>
-static cudaError_t launch_step(psl_grid* g) {
+static cudaError_t launch_step(psl_grid* g, bool held_nu = false) {
   StepParams<S> p;
   p.g = view<S>(g);
   p.marker = g->marker;
@@ -525,14 +533,22 @@ static cudaError_t launch_step(psl_grid* g) {
   p.health = g->health;
   p.ri = row_index<S>(g);
   p.rot = thread_rotation(g);
+  p.nut = g->mlp_nut;
+  p.nu = g->info.nu;
   const unsigned int blocks = blocks_for(g->n, kStepThreads);
   const int addr = 27 * g->f_stride + g->n >= (1ull << 32) ? kAddrView : g->f_twice ? kAddrFlat : kAddrIndex;
   auto launch = [&](auto kernel) { kernel<<<blocks, kStepThreads, 0, g->stream>>>(p); };
   if constexpr (kCollidesOnG<S>) {
-    const bool cs = g->cs_field != nullptr;
-    if (addr == kAddrView) cs ? launch(step_kernel_g<S, kAddrView, true>) : launch(step_kernel_g<S, kAddrView, false>);
-    else if (addr == kAddrFlat) cs ? launch(step_kernel_g<S, kAddrFlat, true>) : launch(step_kernel_g<S, kAddrFlat, false>);
-    else cs ? launch(step_kernel_g<S, kAddrIndex, true>) : launch(step_kernel_g<S, kAddrIndex, false>);
+    const int rate = held_nu ? kRateNuField : g->cs_field ? kRateCsField : kRateUniform;
+    auto pick = [&](auto addr_tag) {
+      constexpr int A = decltype(addr_tag)::value;
+      if (rate == kRateNuField) launch(step_kernel_g<S, A, kRateNuField>);
+      else if (rate == kRateCsField) launch(step_kernel_g<S, A, kRateCsField>);
+      else launch(step_kernel_g<S, A, kRateUniform>);
+    };
+    if (addr == kAddrView) pick(std::integral_constant<int, kAddrView>());
+    else if (addr == kAddrFlat) pick(std::integral_constant<int, kAddrFlat>());
+    else pick(std::integral_constant<int, kAddrIndex>());
   } else {
     if (addr == kAddrView) launch(step_kernel<S, kAddrView>);
     else if (addr == kAddrFlat) launch(step_kernel<S, kAddrFlat>);
@@ -581,7 +597,18 @@ int psl_apply_local_cell_update(psl_grid* g) {
   if (g->mlp) {
     PSL_CHECK(!custom, PSL_ERR_INVALID,
               "psl_apply_local_cell_update: the learned closure does not combine with forcing or moving walls");
-    return psl_detail_launch_learned(g);
+    if (g->mlp_nut && g->mlp_since != 0) {  // between two runs of the closure: its held nu_t
+      PSL_CUDA(with_storage(g->storage, [&](auto s) {
+        using S = decltype(s);
+        if constexpr (kCollidesOnG<S>) return launch_step<S>(g, true);
+        else return cudaErrorInvalidValue;  // the held field exists for 16-bit storage only
+      }));
+    } else {
+      const int rc = psl_detail_launch_learned(g);
+      if (rc != PSL_OK) return rc;
+    }
+    g->mlp_since = (g->mlp_since + 1) % g->mlp_interval;
+    return PSL_OK;
   }
   if (custom) {
     PSL_CHECK(g->storage != kStoreF64 && 27ull * g->f_stride + g->n < (1ull << 32), PSL_ERR_INVALID,
@@ -705,6 +732,7 @@ static int launch_fill_coarse(psl_grid* c, psl_grid* f) {
 
 int psl_fill_coarse_grid_from_fine(psl_grid* c, psl_grid* f) {
   PSL_CHECK(c && f, PSL_ERR_INVALID, "psl_fill_coarse_grid_from_fine: null grid");
+  psl_detail_closure_stale(c);
   PSL_CHECK(c->storage == f->storage, PSL_ERR_INVALID,
             "psl_fill_coarse_grid_from_fine: coarse and fine grids use different storage");
   const psl_info& C = c->info;
@@ -912,6 +940,7 @@ int psl_get_macroscopic(psl_grid* g, double* host) {
 
 int psl_set_populations(psl_grid* g, const float* host) {
   PSL_CHECK(g && host, PSL_ERR_INVALID, "psl_set_populations: null argument");
+  psl_detail_closure_stale(g);
   DeviceGuard dg(g->device);
   PSL_CUDA(cudaStreamSynchronize(g->stream));
   return with_storage(g->storage, [&](auto s) { return scatter<decltype(s)>(g, host); });
@@ -925,6 +954,7 @@ int psl_get_shifts(const psl_grid* g, int* s) {
 
 int psl_set_shifts(psl_grid* g, const int* s) {
   PSL_CHECK(g && s, PSL_ERR_INVALID, "psl_set_shifts: null argument");
+  psl_detail_closure_stale(g);
   for (int q = 0; q < 27; ++q)
     PSL_CHECK(s[q] >= 0 && (uint32_t)s[q] < g->n, PSL_ERR_INVALID, "psl_set_shifts: shift outside [0, N)");
   for (int q = 0; q < 27; ++q) g->shift[q] = (uint32_t)s[q];

@@ -58,7 +58,14 @@ struct psl_grid {
   void* mlp = nullptr;              // learned closure (psl::MlpDevice), or null: Smagorinsky
   float mlp_width = 1.f;            // filter width fed to the closure
   float mlp_scalars[24] = {};       // its normalisation, b3, output scale (psl::MlpScalars)
+  int mlp_interval = 1;             // the closure runs on every mlp_interval-th update (16-bit storage)
+  int mlp_since = 0;                // updates since its last run; 0: the next update runs it
+  uint16_t* mlp_nut = nullptr;      // per-cell FP16 nu_t of its last run (mlp_interval > 1), or null
 };
+
+// Marks the held nu_t of the learned closure as out of date, so that the next update
+// evaluates the closure (after populations or markers were set from outside the update).
+inline void psl_detail_closure_stale(psl_grid* g) { g->mlp_since = 0; }
 
 // Thread-to-cell rotation of the update kernels (psl_capi.cu, cell_of_thread in
 // psl_kernels.cuh).

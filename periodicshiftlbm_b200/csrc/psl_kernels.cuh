@@ -62,7 +62,17 @@ struct StepParams {
   RelaxationT<typename S::calc> rx;
   unsigned int* health;  // bit 0 set when a collided cell's density is not finite/positive
   uint32_t rot;          // thread-to-cell rotation (cell_of_thread)
+  const uint16_t* nut;   // per-cell FP16 eddy viscosity held from the learned closure's last
+                         // evaluation (kRateNuField), or null
+  float nu;              // the grid's lattice viscosity (kRateNuField)
 };
+
+// Relaxation rate of the 16-bit update kernel:
+//   kRateUniform   Smagorinsky with the grid's constant
+//   kRateCsField   Smagorinsky with the cell's constant (p.cs)
+//   kRateNuField   omega = 1 / (3 (nu + nu_t) + 1/2) with the cell's held nu_t (p.nut), the
+//                  learned closure's rate between two of its evaluations
+enum RateKind : int { kRateUniform = 0, kRateCsField = 1, kRateNuField = 2 };
 
 // Cell of thread t: t - rot, cyclically.  With rot = 16 and Nx a multiple of 32, the last
 // cell of one x-row and the first of the next (both x-face cells, i = Nx - 1 and i = 0) fall
@@ -281,7 +291,7 @@ __device__ __forceinline__ void update_one_cell(const StepParams<S>& p, uint32_t
 // allocator: the loads and the collision run on every lane and only the stores are
 // predicated, instead of early returns (which cost ~50 spilled registers at the 64-register
 // cap).  `cell` must be < N.
-template <typename S, int kAddr, bool kCsField>
+template <typename S, int kAddr, int kRate>
 __device__ __forceinline__ void update_one_cell_g(const StepParams<S>& p, uint32_t cell, uint8_t m, float* slot) {
   using B = StoredBits<S>;
   const int kind = marker_kind(m);
@@ -300,6 +310,8 @@ __device__ __forceinline__ void update_one_cell_g(const StepParams<S>& p, uint32
   // past the grid on cell 0 -- computes on real values and stores nothing): cheaper than
   // predicating the loads and zeroing the rest
   load_for<B, kAddr>(p, cell, h);
+  // the kept nu_t, loaded with the populations (every lane: cell < N)
+  const uint16_t nut_bits = kRate == kRateNuField ? __ldg(p.nut + cell) : (uint16_t)0;
   const bool collides = kind != kSkip && kind != kSolid;
   float g[27];
   CellMomentsG cm;
@@ -321,8 +333,15 @@ __device__ __forceinline__ void update_one_cell_g(const StepParams<S>& p, uint32
     cm = cell_moments_g(g);
   }
   if (collides && p.health && !finite_density(cm.rho)) atomicOr(p.health, 1u);
-  const float cs18 = kCsField && collides ? 18.f * p.cs[cell] : p.rx.cs18;
-  relax_rebuild_g(g, cm, smagorinsky_omega_g(cm, p.rx.omega0, p.rx.tau, p.rx.tau2, cs18));
+  float omega;
+  if constexpr (kRate == kRateNuField) {
+    const float nu_t = __half2float(__ushort_as_half(nut_bits));
+    omega = grecip(3.f * (p.nu + nu_t) + 0.5f);  // the learned closure's expression (psl_learned.cuh)
+  } else {
+    const float cs18 = kRate == kRateCsField && collides ? 18.f * p.cs[cell] : p.rx.cs18;
+    omega = smagorinsky_omega_g(cm, p.rx.omega0, p.rx.tau, p.rx.tau2, cs18);
+  }
+  relax_rebuild_g(g, cm, omega);
   if (collides) store_for<StoredOf<S>, kAddr>(p, cell, g);
 }
 
@@ -339,8 +358,8 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constan
 // One thread per cell: the 16-bit forms, held to 64 registers (8 blocks of 128 per SM;
 // 4 with 64-bit row pointers).  Left free the compiler hoists loads into 96 registers and
 // the lower occupancy costs more than the hoisting gains.
-// kCsField: the grid has a per-cell Smagorinsky field (p.cs), else the uniform constant.
-template <typename S, int kAddr, bool kCsField>
+// kRate: where the relaxation rate comes from (RateKind).
+template <typename S, int kAddr, int kRate>
 __global__ void __launch_bounds__(kStepThreads, kAddr == kAddrView ? 4 : 8) step_kernel_g(const __grid_constant__ StepParams<S> p) {
   static_assert(kCollidesOnG<S>, "FP32 / FP64 storage runs step_kernel");
   __shared__ float slot[kStepThreads][27];
@@ -349,7 +368,7 @@ __global__ void __launch_bounds__(kStepThreads, kAddr == kAddrView ? 4 : 8) step
   const uint32_t cell = in ? cell_of_thread(t, p.rot, p.g.n) : 0u;
   const uint8_t m = in ? p.marker[cell] : make_marker(kSkip, 0);
   if (__all_sync(0xffffffffu, marker_kind(m) == kSkip)) return;  // ghost layers, refined interior
-  update_one_cell_g<S, kAddr, kCsField>(p, cell, m, slot[threadIdx.x]);
+  update_one_cell_g<S, kAddr, kRate>(p, cell, m, slot[threadIdx.x]);
 }
 
 // ------------------------------------------------------------------------------------------

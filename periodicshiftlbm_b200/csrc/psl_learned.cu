@@ -125,11 +125,17 @@ int launch(psl_grid* g) {
   p.n = g->n;
   p.health = g->health;
   p.rot = psl_detail_thread_rotation(g);
+  p.nut = g->mlp_nut;
   const unsigned int blocks = (g->n + kStepThreads - 1) / kStepThreads;
-  if (g->f_twice)
-    step_learned_warp_kernel<S, true><<<blocks, kStepThreads, 0, g->stream>>>(p);
-  else
-    step_learned_warp_kernel<S, false><<<blocks, kStepThreads, 0, g->stream>>>(p);
+  auto go = [&](auto kernel) { kernel<<<blocks, kStepThreads, 0, g->stream>>>(p); };
+  if constexpr (kCollidesOnG<S>) {
+    if (g->mlp_nut) {  // evaluated every mlp_interval-th update: keep nu_t for the others
+      g->f_twice ? go(step_learned_warp_kernel<S, true, true>) : go(step_learned_warp_kernel<S, false, true>);
+      MLP_CUDA(cudaGetLastError());
+      return PSL_OK;
+    }
+  }
+  g->f_twice ? go(step_learned_warp_kernel<S, true, false>) : go(step_learned_warp_kernel<S, false, false>);
   MLP_CUDA(cudaGetLastError());
   return PSL_OK;
 }
@@ -148,6 +154,7 @@ int psl_detail_launch_learned(psl_grid* g) {
 int psl_set_sgs_mlp(psl_grid* g, const psl_sgs_mlp* mlp, float filter_width) {
   if (!g) return fail(PSL_ERR_INVALID, "psl_set_sgs_mlp: null grid");
   DeviceGuard dg(g->device);
+  psl_detail_closure_stale(g);
   if (!mlp) {
     if (g->mlp) {
       MLP_CUDA(cudaStreamSynchronize(g->stream));
@@ -173,6 +180,31 @@ int psl_set_sgs_mlp(psl_grid* g, const psl_sgs_mlp* mlp, float filter_width) {
   MLP_CUDA(cudaStreamSynchronize(g->stream));
   g->mlp_width = filter_width;
   std::memcpy(g->mlp_scalars, &sc, sizeof(MlpScalars));
+  return PSL_OK;
+}
+
+int psl_set_sgs_mlp_interval(psl_grid* g, int interval) {
+  if (!g) return fail(PSL_ERR_INVALID, "psl_set_sgs_mlp_interval: null grid");
+  if (interval < 1) return fail(PSL_ERR_INVALID, "psl_set_sgs_mlp_interval: the interval must be at least 1");
+  if (interval > 1 && g->storage != kStoreF16 && g->storage != kStoreBF16)
+    return fail(PSL_ERR_INVALID, "psl_set_sgs_mlp_interval: intervals above 1 need FP16 or BF16 storage");
+  DeviceGuard dg(g->device);
+  if (interval == 1) {
+    if (g->mlp_nut) {
+      MLP_CUDA(cudaStreamSynchronize(g->stream));
+      cudaFree(g->mlp_nut);
+      g->mlp_nut = nullptr;
+    }
+  } else if (!g->mlp_nut) {
+    cudaError_t e = cudaMalloc(&g->mlp_nut, (size_t)g->n * sizeof(uint16_t));
+    if (e != cudaSuccess) {
+      g->mlp_nut = nullptr;
+      cudaGetLastError();
+      return fail(PSL_ERR_NOMEM, std::string("psl_set_sgs_mlp_interval: ") + cudaGetErrorString(e));
+    }
+  }
+  g->mlp_interval = interval;
+  psl_detail_closure_stale(g);
   return PSL_OK;
 }
 

@@ -32,6 +32,8 @@ struct LearnedParams {
   uint32_t n;
   unsigned int* health;
   uint32_t rot;              // thread-to-cell rotation (cell_of_thread)
+  uint16_t* nut;             // kStoreNu: each collided cell's nu_t as FP16, held for the updates
+                             // until the next evaluation (step_kernel_g, kRateNuField)
 };
 
 // The closure's features from D = C - rho/3 I (the g-form moments): the same quantities
@@ -73,8 +75,9 @@ __device__ __forceinline__ void store_rows(const RowIndex<S>& r, uint32_t cell, 
 
 // 7 blocks of 128 per SM (72 registers; ptxas keeps ~40 bytes in local memory, L1-resident):
 // 1.2% faster than 6 blocks at 80 registers without spills, measured on the sphere case.
-template <typename S, bool kFlat>
+template <typename S, bool kFlat, bool kStoreNu>
 __global__ void __launch_bounds__(kStepThreads, 7) step_learned_warp_kernel(const __grid_constant__ LearnedParams<S> p) {
+  static_assert(!kStoreNu || kCollidesOnG<S>, "the held nu_t field serves the 16-bit update only");
   __shared__ __align__(16) float bc_slot[kStepThreads][27];
   // the warp's FP16 feature tile lives in its own lanes' boundary slots (free after the
   // __syncwarp that follows every lane's boundary condition)
@@ -126,6 +129,7 @@ __global__ void __launch_bounds__(kStepThreads, 7) step_learned_warp_kernel(cons
     __syncwarp();
     const float nu_t = mlp_warp_eval(p.mlpw, p.sc, xt, x);
     if (collides) {
+      if constexpr (kStoreNu) p.nut[cell] = __half_as_ushort(__float2half_rn(nu_t));
       relax_rebuild_g(f, cm, grecip(3.f * (p.nu + nu_t) + 0.5f));
       store_rows<StoredOf<S>, kFlat>(p.ri, cell, f);
     }

@@ -15,7 +15,9 @@ included, and a mean is comparable only over several shedding periods.
 
 A form "<storage>+mlp" runs that storage with the learned closure (the packaged weights,
 periodicshiftlbm_b200/data) in place of Smagorinsky; its errors against the FP64
-(Smagorinsky) run then hold the model difference as well as the rounding.
+(Smagorinsky) run then hold the model difference as well as the rounding.  "<storage>+mlpK"
+(16-bit storage) runs the closure's network on every K-th update only, each cell relaxing
+with its kept nu_t in between (psl_set_sgs_mlp_interval).
 
 ``python -m periodicshiftlbm_b200.precision --scale 0.5 --steps 5000`` runs the
 256x128x128 two-level subsample of the 512x256x256 Re=1e5 sphere case.
@@ -66,12 +68,13 @@ def run_form(cfg: SphereConfig, storage: str, steps: int, sample_every: int = 50
     grids."""
     storage, _, closure = storage.partition("+")
     grids, case = make_sphere_grids(cfg, storage=storage)
-    if closure == "mlp":
+    if closure.startswith("mlp"):
         from .sgs import load_params, set_sgs_mlp
 
         params = load_params()
+        interval = int(closure[3:] or 1)
         for g in grids:
-            set_sgs_mlp(g, params, g.Info.res / grids[0].Info.res)
+            set_sgs_mlp(g, params, g.Info.res / grids[0].Info.res, interval=interval if interval > 1 else None)
     fine = grids[-1]
     drags = []
     t0 = time.perf_counter()

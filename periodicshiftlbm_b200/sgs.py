@@ -34,13 +34,23 @@ def from_c(m: PslSgsMlp) -> dict:
     return out
 
 
-def set_sgs_mlp(grid, p: dict | None, filter_width: float = 1.0):
-    """Use the closure in the grid's update kernel (None: back to Smagorinsky)."""
+def set_sgs_mlp(grid, p: dict | None, filter_width: float = 1.0, interval: int | None = None):
+    """Use the closure in the grid's update kernel (None: back to Smagorinsky).  `interval`
+    (psl_set_sgs_mlp_interval): run the network on every interval-th update only and relax
+    with each cell's kept nu_t in between (FP16 / BF16 storage); None keeps the grid's
+    setting (1 unless set)."""
     if p is None:
         call("psl_set_sgs_mlp", grid.handle, None, ctypes.c_float(filter_width))
     else:
         m = to_c(p)
         call("psl_set_sgs_mlp", grid.handle, ctypes.byref(m), ctypes.c_float(filter_width))
+    if interval is not None:
+        set_sgs_mlp_interval(grid, interval)
+
+
+def set_sgs_mlp_interval(grid, interval: int):
+    """psl_set_sgs_mlp_interval: the closure runs on every `interval`-th update of the grid."""
+    call("psl_set_sgs_mlp_interval", grid.handle, int(interval))
 
 
 def mlp_infer(p: dict, x: np.ndarray) -> np.ndarray:

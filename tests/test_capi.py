@@ -62,6 +62,8 @@ def test_null_grid_arguments_rejected():
     assert L.psl_apply_coarse_fine_grid_communication(None, None) == 1
     assert L.psl_sphere_force_async(None, None, None) == 1
     assert L.psl_grid_get_layout(None, None, None) == 1
+    assert L.psl_set_sgs_mlp_interval(None, 2) == 1
+    assert b"null grid" in L.psl_last_error()
 
 
 def test_unknown_grid_flags_rejected():

@@ -6,7 +6,7 @@ import pytest
 from gpu_helpers import rel
 from oracle import mlp_oracle as mo
 from periodicshiftlbm_b200 import GridStruct, InfoStruct, applyLocalCellUpdate, applyStreaming, fillEquilibriumFromFunction
-from periodicshiftlbm_b200.sgs import mlp_infer, set_sgs_mlp
+from periodicshiftlbm_b200.sgs import mlp_infer, set_sgs_mlp, set_sgs_mlp_interval
 
 pytestmark = pytest.mark.gpu
 
@@ -101,6 +101,97 @@ def test_fused_learned_update_matches_oracle_cell_by_cell(orc, storage, path):
         w = np.array([8 / 27] + [2 / 27] * 6 + [1 / 54] * 12 + [1 / 216] * 8)[:, None]
         bound = 2e-3 if storage == "f16" else 1.6e-2
         assert np.max(np.abs(f_out[:, idx] - want) / np.maximum(np.abs(want - w), 1e-4)) < bound
+    g.close()
+
+
+W_LATTICE = np.array([8 / 27] + [2 / 27] * 6 + [1 / 54] * 12 + [1 / 216] * 8)[:, None]
+
+
+def _check_against_oracle(orc, storage, f_in, f_out, nu_t, idx):
+    """f_out[:, idx] is the oracle collision of f_in[:, idx] at viscosity 0.01 + nu_t, within
+    the bound of the stored 16-bit f - w (as the fused-update test)."""
+    want = np.stack([orc.collision(f_in[:, c], float(np.float32(0.01) + np.float32(nu_t[c])), 0.0) for c in idx],
+                    axis=1)
+    bound = 2e-3 if storage == "f16" else 1.6e-2
+    err = np.max(np.abs(f_out[:, idx] - want) / np.maximum(np.abs(want - W_LATTICE), 1e-4))
+    assert err < bound, err
+
+
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+def test_closure_interval_first_update_equals_every_update(storage):
+    """With an interval the first update still runs the network: the same bits as the
+    closure on every update."""
+    p = mo.random_params(5)
+    a = periodic_grid(storage=storage)
+    b = periodic_grid(storage=storage)
+    set_sgs_mlp(a, p, 1.0)
+    set_sgs_mlp(b, p, 1.0, interval=3)
+    for g in (a, b):
+        applyStreaming(g)
+        applyLocalCellUpdate(g)
+    assert np.array_equal(a.fArray, b.fArray)
+    for g in (a, b):
+        assert g.health() == 0
+        g.close()
+
+
+@pytest.mark.parametrize("path", ["whole", "partial"])
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+def test_closure_interval_updates_use_the_kept_nu_t(orc, storage, path):
+    """Interval 3: updates 1 and 4 run the network on their own input; updates 2 and 3
+    relax with the nu_t of update 1's input, kept in FP16."""
+    p = mo.random_params(5)
+    g = periodic_grid(storage=storage, n=SHAPES[path], nu=0.01)
+    set_sgs_mlp(g, p, 1.0, interval=3)
+    idx = np.random.default_rng(1).choice(g.cellCount, 200, replace=False)
+    kept = None
+    for step in range(4):
+        applyStreaming(g)
+        f_in = g.fArray
+        applyLocalCellUpdate(g)
+        f_out = g.fArray
+        if step % 3 == 0:
+            nu_t = mo.forward_device(p, mo.features(f_in, 1.0).astype(np.float32))
+            kept = nu_t.astype(np.float16).astype(np.float32)
+        else:
+            nu_t = kept
+        _check_against_oracle(orc, storage, f_in, f_out, nu_t, idx)
+    assert g.health() == 0
+    g.close()
+
+
+def test_closure_interval_restarts_after_new_populations():
+    """Setting populations from outside makes the next update run the network again."""
+    p = mo.random_params(7)
+    a = periodic_grid(storage="f16", seed=3)
+    b = periodic_grid(storage="f16", seed=3)
+    set_sgs_mlp(a, p, 1.0, interval=4)
+    set_sgs_mlp(b, p, 1.0)
+    applyStreaming(a)
+    applyLocalCellUpdate(a)           # runs the network; the next three would not
+    b.shifter = a.shifter             # both at the same shifts and state
+    b.fArray = a.fArray
+    a.fArray = a.fArray               # a fresh state set from outside
+    for g in (a, b):
+        applyStreaming(g)
+        applyLocalCellUpdate(g)
+    assert np.array_equal(a.fArray, b.fArray)
+    set_sgs_mlp_interval(a, 1)        # back to every update: the kept field is released
+    for g in (a, b):
+        applyStreaming(g)
+        applyLocalCellUpdate(g)
+    assert np.array_equal(a.fArray, b.fArray)
+    a.close()
+    b.close()
+
+
+def test_closure_interval_needs_16_bit_storage():
+    g = periodic_grid(storage="f32")
+    with pytest.raises(Exception, match="FP16 or BF16"):
+        set_sgs_mlp_interval(g, 2)
+    with pytest.raises(Exception, match="at least 1"):
+        set_sgs_mlp_interval(g, 0)
+    set_sgs_mlp_interval(g, 1)
     g.close()
 
 

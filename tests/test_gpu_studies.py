@@ -46,16 +46,18 @@ def test_spectrum_study_reduced():
     assert abs(e["closure_f16"] / e["closure_f32"] - 1) < 0.01, e
 
 
-def test_closure_drag_tracks_plain_fp32_over_many_periods():
-    """The FP16 + closure form against the plain FP32 form on the quarter-scale refined
-    sphere: mean drag coefficient over the second half of 20,000 coarse steps (several
-    shedding periods; the instantaneous drag of the unsteady wake swings by several percent
-    and runs that differ in rounding drift apart in phase, so only long means compare).
-    Measured: 1.6% (20,000 steps) and 0.5% (40,000 steps) apart; FP32 itself sits 0.3-1.5%
-    from the FP64 run."""
-    res = precision.study(config2(scale=0.25), steps=20000, forms=("f32", "f16+mlp"), sample_every=20,
+@pytest.mark.parametrize("form", ["f16+mlp", "f16+mlp4"])
+def test_closure_drag_tracks_plain_fp32_over_many_periods(form):
+    """The FP16 + closure form (f16+mlp4: the network on every fourth update, the kept nu_t
+    in between) against the plain FP32 form on the quarter-scale refined sphere: mean drag
+    coefficient over the second half of 20,000 coarse steps (several shedding periods; the
+    instantaneous drag of the unsteady wake swings by several percent and runs that differ
+    in rounding drift apart in phase, so only long means compare).  Measured for f16+mlp:
+    1.6% (20,000 steps) and 0.5% (40,000 steps) apart; FP32 itself sits 0.3-1.5% from the
+    FP64 run."""
+    res = precision.study(config2(scale=0.25), steps=20000, forms=("f32", form), sample_every=20,
                           average_last=0.5)
     f = res["forms"]
-    cd32, cd16m = f["f32"]["cd_mean"], f["f16+mlp"]["cd_mean"]
+    cd32, cd16m = f["f32"]["cd_mean"], f[form]["cd_mean"]
     assert abs(cd16m / cd32 - 1) < 0.03, (cd16m, cd32)
-    assert all(h == 0 for h in f["f16+mlp"]["health"])
+    assert all(h == 0 for h in f[form]["health"])

@@ -248,6 +248,7 @@ def measure_form(args, cfg, storage: str, sgs: str, world: int, local: int, with
         applyStreaming,
         getSphereForce,
         getSphereForceAsync,
+        updateGrid,
     )
     from periodicshiftlbm_b200.cases import make_sphere_grids
 
@@ -290,8 +291,11 @@ def measure_form(args, cfg, storage: str, sgs: str, world: int, local: int, with
 
             dist.barrier()
 
+    # the timed steps: updateGrid, one library call per coarse step (psl_update_grid, which
+    # updates the coarse cells away from the refinement block on a side stream beside the fine
+    # updates and the transfer)
     for _ in range(args.warmup):
-        update(0, False)
+        updateGrid(grids, 0)
     torch.cuda.synchronize()
     barrier()
     sampler = ClockSampler(local)
@@ -299,12 +303,17 @@ def measure_form(args, cfg, storage: str, sgs: str, world: int, local: int, with
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0.record(stream)
     for _ in range(args.steps):
-        update(0, True)
+        updateGrid(grids, 0)
     t1.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
     barrier()
     ms = max_over_ranks(t0.elapsed_time(t1), world)
+    # the update kernels' own launch times: CUDA events around each update launch in a few
+    # serial steps right after the timed ones (one launch at a time on the grids' stream)
+    for _ in range(min(args.steps, 8)):
+        update(0, True)
+    torch.cuda.synchronize()
     updates = cfg.updates_per_step()
     drag_after = float(getSphereForce(grids[-1], case)[0])
     out = {
@@ -367,7 +376,7 @@ def measure_form(args, cfg, storage: str, sgs: str, world: int, local: int, with
         for g, h in zip(grids, pinned_in):
             g.write_populations(h.numpy())
         for s in range(args.steps):
-            update(0, False)
+            updateGrid(grids, 0)
             getSphereForceAsync(grids[-1], case, drag_hist.data_ptr() + s * 24)
         # the reference driver's output (flowAroundSphereMainSingle.cu:266-277): the coarse
         # levels filled from the fine ones, then the XY section at mid-height of every level
@@ -427,7 +436,9 @@ def run_native(args):
         "config": config_dict(cfg, args.storage, args.sgs, world, args.sgs_interval),
         "roofline": main["roofline"],
         "e2e": main["e2e"],
-        "gpu_launches": args.steps * (1 + 3 * (levels - 1)),
+        # per coarse step on two levels: the coarse update as two launches (near slab, far
+        # layers), two fine updates, the transfer as two launches (restriction, prolongation)
+        "gpu_launches": args.steps * (6 if levels == 2 else 1 + 3 * (levels - 1)),
         "clocks": main["clocks"],
         "drag_after_timed": main["drag_after_timed"],
         "drag_last": main.get("drag_last"),

@@ -61,6 +61,11 @@ struct psl_grid {
   int mlp_interval = 1;             // the closure runs on every mlp_interval-th update (16-bit storage)
   int mlp_since = 0;                // updates since its last run; 0: the next update runs it
   uint16_t* mlp_nut = nullptr;      // per-cell FP16 nu_t of its last run (mlp_interval > 1), or null
+  // psl_update_grid's concurrent schedule (the coarse cells away from the refinement block
+  // updated beside the fine updates and the transfer): a low-priority side stream and its
+  // events, created on first use, or null
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_near = nullptr, ev_far = nullptr;
 };
 
 // Marks the held nu_t of the learned closure as out of date, so that the next update
@@ -72,5 +77,8 @@ inline void psl_detail_closure_stale(psl_grid* g) { g->mlp_since = 0; }
 __attribute__((visibility("hidden"))) uint32_t psl_detail_thread_rotation(const psl_grid* g);
 
 // Launches the update kernel with the learned closure (psl_learned.cu); status as psl_*.
-__attribute__((visibility("hidden"))) int psl_detail_launch_learned(psl_grid* g);
+namespace psl {
+struct ThreadRange;
+}
+__attribute__((visibility("hidden"))) int psl_detail_launch_learned(psl_grid* g, const psl::ThreadRange& range);
 

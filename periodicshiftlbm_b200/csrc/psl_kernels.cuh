@@ -51,6 +51,17 @@ struct RowIndex {
 };
 
 
+// The threads of an update launch: launch thread u (u < count) is thread
+// t_begin + u + (u >= gap_at ? gap_len : 0) of cell_of_thread, so one launch can run a
+// contiguous range of threads, or all threads but one contiguous range.
+struct ThreadRange {
+  uint32_t t_begin, gap_at, gap_len, count;
+};
+__host__ __device__ inline ThreadRange full_range(uint32_t n) { return ThreadRange{0u, 0xffffffffu, 0u, n}; }
+__device__ __forceinline__ uint32_t range_thread(const ThreadRange& r, uint32_t u) {
+  return r.t_begin + u + (u >= r.gap_at ? r.gap_len : 0u);
+}
+
 template <typename S>
 struct StepParams {
   GridView<S> g;
@@ -65,6 +76,7 @@ struct StepParams {
   const uint16_t* nut;   // per-cell FP16 eddy viscosity held from the learned closure's last
                          // evaluation (kRateNuField), or null
   float nu;              // the grid's lattice viscosity (kRateNuField)
+  ThreadRange range;     // the threads of cell_of_thread this launch runs
 };
 
 // Relaxation rate of the 16-bit update kernel:
@@ -349,9 +361,9 @@ __device__ __forceinline__ void update_one_cell_g(const StepParams<S>& p, uint32
 template <typename S, int kAddr>
 __global__ void __launch_bounds__(kStepThreads) step_kernel(const __grid_constant__ StepParams<S> p) {
   static_assert(!kCollidesOnG<S>, "16-bit storage runs step_kernel_g");
-  const uint32_t t = blockIdx.x * kStepThreads + threadIdx.x;
-  if (t >= p.g.n) return;
-  const uint32_t cell = cell_of_thread(t, p.rot, p.g.n);
+  const uint32_t u = blockIdx.x * kStepThreads + threadIdx.x;
+  if (u >= p.range.count) return;
+  const uint32_t cell = cell_of_thread(range_thread(p.range, u), p.rot, p.g.n);
   update_one_cell<S, kAddr>(p, cell, p.marker[cell]);
 }
 
@@ -363,9 +375,9 @@ template <typename S, int kAddr, int kRate>
 __global__ void __launch_bounds__(kStepThreads, kAddr == kAddrView ? 4 : 8) step_kernel_g(const __grid_constant__ StepParams<S> p) {
   static_assert(kCollidesOnG<S>, "FP32 / FP64 storage runs step_kernel");
   __shared__ float slot[kStepThreads][27];
-  const uint32_t t = blockIdx.x * kStepThreads + threadIdx.x;
-  const bool in = t < p.g.n;
-  const uint32_t cell = in ? cell_of_thread(t, p.rot, p.g.n) : 0u;
+  const uint32_t u = blockIdx.x * kStepThreads + threadIdx.x;
+  const bool in = u < p.range.count;
+  const uint32_t cell = in ? cell_of_thread(range_thread(p.range, u), p.rot, p.g.n) : 0u;
   const uint8_t m = in ? p.marker[cell] : make_marker(kSkip, 0);
   if (__all_sync(0xffffffffu, marker_kind(m) == kSkip)) return;  // ghost layers, refined interior
   update_one_cell_g<S, kAddr, kRate>(p, cell, m, slot[threadIdx.x]);
@@ -772,7 +784,10 @@ __global__ void __launch_bounds__(kCoarseFineThreads) fill_coarse_kernel(const _
   restrict_cell(p.c, p.f, p, p.iS + 1 + (int)(t % a), p.jS + 1 + (int)((t / a) % b), p.kS + 1 + (int)(t / (a * b)));
 }
 
-template <typename S>
+// kPhase 0: both phases in one cooperative launch with the grid barrier between them;
+// 1: the restriction alone, 2: the prolongation alone, as two ordinary launches in stream
+// order (the launch boundary is the barrier), which share the SMs with concurrent kernels.
+template <typename S, int kPhase = 0>
 __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const __grid_constant__ CoarseFineParams<S> p) {
   using T = typename S::calc;
   // The row offsets of both grids are read from shared memory inside the item loops (kept
@@ -792,7 +807,7 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
   }
   __syncthreads();
   // ---------------- phase 1: restriction ----------------
-  {
+  if (kPhase != 2) {
     const int a = p.iE - p.iS - 2, b = p.jE - p.jS - 2, c = p.kE - p.kS - 2;  // ring box extents
     const uint32_t faceK = 2u * a * b;
     const uint32_t faceJ = 2u * a * (c - 2);
@@ -819,7 +834,8 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
       restrict_cell(rc, rf, p, p.iS + 1 + ri, p.jS + 1 + rj, p.kS + 1 + rk);
     }
   }
-  grid_barrier(p.barrier, p.nblocks, p.error);
+  if (kPhase == 1) return;
+  if (kPhase == 0) grid_barrier(p.barrier, p.nblocks, p.error);
   // ---------------- phase 2: prolongation ----------------
   const uint32_t kPos[3] = {dir_mask(0, 1), dir_mask(1, 1), dir_mask(2, 1)};
   const uint32_t kNeg[3] = {dir_mask(0, -1), dir_mask(1, -1), dir_mask(2, -1)};

@@ -103,7 +103,7 @@ void pack(const psl_sgs_mlp& m, MlpDevice& d) {
 }
 
 template <typename S>
-int launch(psl_grid* g) {
+int launch(psl_grid* g, const ThreadRange& range) {
   const MlpBoth* both = static_cast<const MlpBoth*>(g->mlp);
   MlpScalars sc;
   std::memcpy(&sc, g->mlp_scalars, sizeof(MlpScalars));
@@ -126,7 +126,8 @@ int launch(psl_grid* g) {
   p.health = g->health;
   p.rot = psl_detail_thread_rotation(g);
   p.nut = g->mlp_nut;
-  const unsigned int blocks = (g->n + kStepThreads - 1) / kStepThreads;
+  p.range = range;
+  const unsigned int blocks = (range.count + kStepThreads - 1) / kStepThreads;
   auto go = [&](auto kernel) { kernel<<<blocks, kStepThreads, 0, g->stream>>>(p); };
   if constexpr (kCollidesOnG<S>) {
     if (g->mlp_nut) {  // evaluated every mlp_interval-th update: keep nu_t for the others
@@ -142,11 +143,11 @@ int launch(psl_grid* g) {
 
 }  // namespace
 
-int psl_detail_launch_learned(psl_grid* g) {
+int psl_detail_launch_learned(psl_grid* g, const ThreadRange& range) {
   switch (g->storage) {
-    case kStoreF32: return launch<StoreF32>(g);
-    case kStoreF16: return launch<StoreF16>(g);
-    case kStoreBF16: return launch<StoreBF16>(g);
+    case kStoreF32: return launch<StoreF32>(g, range);
+    case kStoreF16: return launch<StoreF16>(g, range);
+    case kStoreBF16: return launch<StoreBF16>(g, range);
     default: return fail(PSL_ERR_INVALID, "learned update: FP64 storage is for oracle runs only");
   }
 }

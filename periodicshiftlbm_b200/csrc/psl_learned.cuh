@@ -34,6 +34,7 @@ struct LearnedParams {
   uint32_t rot;              // thread-to-cell rotation (cell_of_thread)
   uint16_t* nut;             // kStoreNu: each collided cell's nu_t as FP16, held for the updates
                              // until the next evaluation (step_kernel_g, kRateNuField)
+  ThreadRange range;         // the threads of cell_of_thread this launch runs
 };
 
 // The closure's features from D = C - rho/3 I (the g-form moments): the same quantities
@@ -82,9 +83,9 @@ __global__ void __launch_bounds__(kStepThreads, 7) step_learned_warp_kernel(cons
   // the warp's FP16 feature tile lives in its own lanes' boundary slots (free after the
   // __syncwarp that follows every lane's boundary condition)
   __half* xt = reinterpret_cast<__half*>(&bc_slot[threadIdx.x & ~31u][0]);
-  const uint32_t t = blockIdx.x * kStepThreads + threadIdx.x;
-  const bool in = t < p.n;
-  const uint32_t cell = in ? cell_of_thread(t, p.rot, p.n) : 0u;
+  const uint32_t u = blockIdx.x * kStepThreads + threadIdx.x;
+  const bool in = u < p.range.count;
+  const uint32_t cell = in ? cell_of_thread(range_thread(p.range, u), p.rot, p.n) : 0u;
   const uint8_t m = in ? p.marker[cell] : make_marker(kSkip, 0);
   const int kind = marker_kind(m);
   float x[kMlpIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};

@@ -371,8 +371,8 @@ int psl_set_populations(psl_grid* grid, const float* host);
 int psl_get_shifts(const psl_grid* grid, int* shifts27);
 int psl_set_shifts(psl_grid* grid, const int* shifts27);
 int psl_synchronize(psl_grid* grid);
-/* Health word of the update kernels (bit 0: non-finite density seen; bit 1: a grid
- * barrier timed out; bit 2: a wait of the learned closure timed out); read and clear. */
+/* Health word of the update kernels (bit 0: non-finite density seen; bit 2: a wait of the
+ * learned closure timed out; bit 1 is not used); read and clear. */
 int psl_check_health(psl_grid* grid, unsigned int* flags);
 
 /* ---- single-cell entry points (unit parity of the device functions) ----

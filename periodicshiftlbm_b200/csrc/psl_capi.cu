@@ -674,10 +674,8 @@ static int periodic(psl_grid* g, int axis) {
 int psl_apply_bc_periodic_x(psl_grid* g) { return periodic(g, 0); }
 int psl_apply_bc_periodic_y(psl_grid* g) { return periodic(g, 1); }
 
-// split: the restriction and the prolongation as two ordinary launches instead of one
-// cooperative launch with a grid barrier (psl_update_grid's concurrent schedule).
 template <typename S>
-static int launch_coarse_fine(psl_grid* c, psl_grid* f, bool split = false) {
+static int launch_coarse_fine(psl_grid* c, psl_grid* f) {
   const psl_info& C = c->info;
   const psl_info& F = f->info;
   const int a = C.i_subgrid_end - C.i_subgrid_start, b = C.j_subgrid_end - C.j_subgrid_start,
@@ -705,27 +703,11 @@ static int launch_coarse_fine(psl_grid* c, psl_grid* f, bool split = false) {
   p.n_ring = (uint32_t)(ra * rb * rc - (ra - 2) * (rb - 2) * (rc - 2));
   // z faces, y faces, then four lanes per x-row boundary (coarse_fine_kernel)
   p.n_shell = (uint32_t)(4LL * p.fnx * p.fny + 4LL * p.fnx * (p.fnz - 4) + 4LL * (p.fny - 3) * (p.fnz - 4));
-  p.barrier = c->health + 1;
-  p.error = c->health;
-  if (split) {
-    p.nblocks = 0;
-    coarse_fine_kernel<S, 1><<<std::max(1u, blocks_for(p.n_ring, kCoarseFineThreads)), kCoarseFineThreads, 0,
-                               c->stream>>>(p);
-    coarse_fine_kernel<S, 2><<<std::max(1u, blocks_for(p.n_shell, kCoarseFineThreads)), kCoarseFineThreads, 0,
-                               c->stream>>>(p);
-    PSL_CUDA(cudaGetLastError());
-    return PSL_OK;
-  }
-  int sms = 0, per_sm = 0;
-  PSL_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-  PSL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_fine_kernel<S>, kCoarseFineThreads, 0));
-  PSL_CHECK(per_sm > 0, PSL_ERR_CUDA, "coarse/fine: kernel cannot be resident");
-  const unsigned int want = blocks_for(std::max(p.n_ring, p.n_shell), kCoarseFineThreads);
-  p.nblocks = std::min<unsigned int>((unsigned int)(sms * per_sm), std::max(1u, want));
-  PSL_CUDA(cudaMemsetAsync(p.barrier, 0, sizeof(unsigned int), c->stream));
-  void* args[] = {&p};
-  PSL_CUDA(cudaLaunchCooperativeKernel((const void*)coarse_fine_kernel<S>, dim3(p.nblocks), dim3(kCoarseFineThreads),
-                                       args, 0, c->stream));
+  coarse_fine_kernel<S, 1><<<std::max(1u, blocks_for(p.n_ring, kCoarseFineThreads)), kCoarseFineThreads, 0,
+                             c->stream>>>(p);
+  coarse_fine_kernel<S, 2><<<std::max(1u, blocks_for(p.n_shell, kCoarseFineThreads)), kCoarseFineThreads, 0,
+                             c->stream>>>(p);
+  PSL_CUDA(cudaGetLastError());
   return PSL_OK;
 }
 
@@ -774,11 +756,7 @@ int psl_fill_coarse_grid_from_fine(psl_grid* c, psl_grid* f) {
   return with_storage(c->storage, [&](auto s) { return launch_fill_coarse<decltype(s)>(c, f); });
 }
 
-static int coarse_fine(psl_grid* c, psl_grid* f, bool split);
-
-int psl_apply_coarse_fine_grid_communication(psl_grid* c, psl_grid* f) { return coarse_fine(c, f, false); }
-
-static int coarse_fine(psl_grid* c, psl_grid* f, bool split) {
+int psl_apply_coarse_fine_grid_communication(psl_grid* c, psl_grid* f) {
   PSL_CHECK(c && f, PSL_ERR_INVALID, "psl_apply_coarse_fine_grid_communication: null grid");
   PSL_CHECK(c->storage == f->storage, PSL_ERR_INVALID,
             "psl_apply_coarse_fine_grid_communication: coarse and fine grids use different storage");
@@ -793,7 +771,7 @@ static int coarse_fine(psl_grid* c, psl_grid* f, bool split) {
   PSL_CHECK(27ull * c->f_stride + c->n < (1ull << 32) && 27ull * f->f_stride + f->n < (1ull << 32), PSL_ERR_INVALID,
             "coarse/fine: grid too large for 32-bit row offsets");
   DeviceGuard dg(c->device);
-  return with_storage(c->storage, [&](auto s) { return launch_coarse_fine<decltype(s)>(c, f, split); });
+  return with_storage(c->storage, [&](auto s) { return launch_coarse_fine<decltype(s)>(c, f); });
 }
 
 // psl_update_grid's concurrent schedule for the top coarse grid c of a refined hierarchy.
@@ -803,7 +781,7 @@ static int coarse_fine(psl_grid* c, psl_grid* f, bool split) {
 // 27 elements (include/applyLocalCellUpdate.h:34,71), so the far cells share no element with
 // the transfer and none with the fine grid: the near slab runs first on the grid's stream,
 // the far layers then on a low-priority side stream beside the two fine updates and the
-// transfer (restriction and prolongation as ordinary launches, which can share SMs), and
+// transfer (restriction and prolongation: ordinary launches, which can share SMs), and
 // the grid's stream waits for them at the end of the step.  A kernel's launch parameters are fixed
 // when it is queued, so the far launch uses this step's shifts wherever it runs.  The result is the serial
 // schedule's, bit for bit.  Threads [near.t_begin, near.t_begin + near.count) of
@@ -861,7 +839,7 @@ static int concurrent_step(psl_grid** grids, int levels, const ThreadRange& near
   count_update(c);
   PSL_CUDA(cudaEventRecord(c->ev_far, c->side));
   for (int i = 0; i < 2 && rc == PSL_OK; ++i) rc = psl_update_grid(grids, levels, 1);
-  if (rc == PSL_OK) rc = coarse_fine(c, grids[1], true);
+  if (rc == PSL_OK) rc = psl_apply_coarse_fine_grid_communication(c, grids[1]);
   // the grid's stream waits for the far layers, also after a failed fine update or transfer
   const cudaError_t e = cudaStreamWaitEvent(c->stream, c->ev_far, 0);
   if (rc) return rc;

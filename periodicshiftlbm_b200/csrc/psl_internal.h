@@ -46,7 +46,7 @@ struct psl_grid {
   float* cs_field = nullptr;        // per-cell Smagorinsky constants (getSmagorinskyConstant), or null
   uint32_t shift[27] = {};
   cudaStream_t stream = 0;
-  unsigned int* health = nullptr;   // [0] health bits, [1] barrier counter
+  unsigned int* health = nullptr;   // [0] health bits
   double* scratch = nullptr;        // force partials (kForceBlocks x 3) + result (3)
   int device = 0;
   int batched = 0;                  // member of this many live batches (psl_batch.cu)

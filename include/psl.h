@@ -171,8 +171,9 @@ int psl_fill_coarse_grid_from_fine(psl_grid* coarse, psl_grid* fine);
  * streaming + update on grids[level], two steps of level+1, coarse/fine transfer.
  * Kernels go to each grid's stream in call order.  When all levels share one stream and the
  * top grid's refinement block lies at least three cells inside it in z, the top grid's cells
- * away from the block are updated on a low-priority stream of the library's own beside the
- * fine updates and the transfer; the grid's stream waits for them before the call returns,
+ * away from the block are updated on a lowest-priority stream of the library's own beside the
+ * fine updates and the transfer, which run on a highest-priority stream of its own; the
+ * grid's stream waits for both before the call returns,
  * so later work on it sees the whole step, and the result is the serial order's bit for bit
  * (not under stream capture, scalar transport or the customised update: serial order there).
  * The periodic shifts are kernel

@@ -203,12 +203,13 @@ int psl_grid_destroy(psl_grid* g) {
   if (g->givenT) cudaFree(g->givenT);
   if (g->cs_field) cudaFree(g->cs_field);
   if (g->mlp_nut) cudaFree(g->mlp_nut);
-  if (g->side) {
-    cudaStreamSynchronize(g->side);
-    cudaStreamDestroy(g->side);
+  for (cudaStream_t s : {g->side, g->hi}) {
+    if (!s) continue;
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
   }
-  if (g->ev_near) cudaEventDestroy(g->ev_near);
-  if (g->ev_far) cudaEventDestroy(g->ev_far);
+  for (cudaEvent_t e : {g->ev_near, g->ev_far, g->ev_hi})
+    if (e) cudaEventDestroy(e);
   delete g;
   return PSL_OK;
 }
@@ -780,9 +781,9 @@ int psl_apply_coarse_fine_grid_communication(psl_grid* c, psl_grid* f) {
 // kS - 1 .. kE) and the far layers.  In the PS update each cell reads and writes only its own
 // 27 elements (include/applyLocalCellUpdate.h:34,71), so the far cells share no element with
 // the transfer and none with the fine grid: the near slab runs first on the grid's stream,
-// the far layers then on a low-priority side stream beside the two fine updates and the
-// transfer (restriction and prolongation: ordinary launches, which can share SMs), and
-// the grid's stream waits for them at the end of the step.  A kernel's launch parameters are fixed
+// the far layers then on a lowest-priority side stream beside the two fine updates and the
+// transfer (restriction and prolongation: ordinary launches, which can share SMs) on a
+// highest-priority stream, and the grid's stream waits for both at the end of the step.  A kernel's launch parameters are fixed
 // when it is queued, so the far launch uses this step's shifts wherever it runs.  The result is the serial
 // schedule's, bit for bit.  Threads [near.t_begin, near.t_begin + near.count) of
 // cell_of_thread cover the near slab; the far launch runs every other thread.
@@ -815,22 +816,27 @@ static bool concurrent_fits(psl_grid** grids, int levels, ThreadRange& near, Thr
 static int concurrent_step(psl_grid** grids, int levels, const ThreadRange& near, const ThreadRange& far) {
   psl_grid* c = grids[0];
   DeviceGuard dg(c->device);
-  if (!c->side) {
+  if (!c->ev_hi) {
     int least = 0, greatest = 0;
     PSL_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    PSL_CUDA(cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, least));  // the lowest priority
-    PSL_CUDA(cudaEventCreateWithFlags(&c->ev_near, cudaEventDisableTiming));
-    PSL_CUDA(cudaEventCreateWithFlags(&c->ev_far, cudaEventDisableTiming));
+    if (!c->side) PSL_CUDA(cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, least));
+    if (!c->hi) PSL_CUDA(cudaStreamCreateWithPriority(&c->hi, cudaStreamNonBlocking, greatest));
+    if (!c->ev_near) PSL_CUDA(cudaEventCreateWithFlags(&c->ev_near, cudaEventDisableTiming));
+    if (!c->ev_far) PSL_CUDA(cudaEventCreateWithFlags(&c->ev_far, cudaEventDisableTiming));
+    PSL_CUDA(cudaEventCreateWithFlags(&c->ev_hi, cudaEventDisableTiming));
   }
   int rc = psl_apply_streaming(c);
   if (rc) return rc;
   rc = update_cells(c, near);
   if (rc) return rc;
-  // the far layers start once the near slab is done and fill the SMs beside the fine updates
-  // and the transfer (measured: 2.012 against 2.043 ms per FP32 step; started after the fine
-  // updates, beside the transfer alone, 2.021 ms)
+  // Once the near slab is done, the far layers run on the lowest-priority stream and the fine
+  // updates and the transfer on the highest-priority one, whatever the priority of the
+  // grid's own stream: the block scheduler hands SMs to the fine updates first and the far
+  // layers fill in behind them, above all beside the transfer, whose launches alone keep
+  // few warps busy.
   PSL_CUDA(cudaEventRecord(c->ev_near, c->stream));
   PSL_CUDA(cudaStreamWaitEvent(c->side, c->ev_near, 0));
+  PSL_CUDA(cudaStreamWaitEvent(c->hi, c->ev_near, 0));
   cudaStream_t own = c->stream;
   c->stream = c->side;
   rc = update_cells(c, far);
@@ -838,11 +844,16 @@ static int concurrent_step(psl_grid** grids, int levels, const ThreadRange& near
   if (rc) return rc;
   count_update(c);
   PSL_CUDA(cudaEventRecord(c->ev_far, c->side));
+  for (int l = 0; l < levels; ++l) grids[l]->stream = c->hi;
   for (int i = 0; i < 2 && rc == PSL_OK; ++i) rc = psl_update_grid(grids, levels, 1);
   if (rc == PSL_OK) rc = psl_apply_coarse_fine_grid_communication(c, grids[1]);
-  // the grid's stream waits for the far layers, also after a failed fine update or transfer
-  const cudaError_t e = cudaStreamWaitEvent(c->stream, c->ev_far, 0);
+  for (int l = 0; l < levels; ++l) grids[l]->stream = own;
+  // the grid's stream waits for both, also after a failed fine update or transfer
+  cudaError_t e = cudaEventRecord(c->ev_hi, c->hi);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(own, c->ev_hi, 0);
+  const cudaError_t e_far = cudaStreamWaitEvent(own, c->ev_far, 0);
   if (rc) return rc;
+  if (e == cudaSuccess) e = e_far;
   if (e != cudaSuccess) return fail(PSL_ERR_CUDA, std::string("psl_update_grid: ") + cudaGetErrorString(e));
   return PSL_OK;
 }
@@ -894,7 +905,7 @@ static int enqueue_sphere_force(psl_grid* g, const psl_sphere_case* sc, double* 
     launch_force<decltype(s)>(g, i0, j0, k0, si, sj, sk, nb);
     return 0;
   });
-  force_final_kernel<<<1, 32, 0, g->stream>>>(g->scratch, nb, g->scratch + kForceBlocks * 3);
+  force_final_kernel<<<1, 256, 0, g->stream>>>(g->scratch, nb, g->scratch + kForceBlocks * 3);
   PSL_CUDA(cudaGetLastError());
   PSL_CUDA(cudaMemcpyAsync(force3, g->scratch + kForceBlocks * 3, 3 * sizeof(double), kind, g->stream));
   return PSL_OK;

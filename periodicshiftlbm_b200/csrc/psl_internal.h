@@ -62,10 +62,11 @@ struct psl_grid {
   int mlp_since = 0;                // updates since its last run; 0: the next update runs it
   uint16_t* mlp_nut = nullptr;      // per-cell FP16 nu_t of its last run (mlp_interval > 1), or null
   // psl_update_grid's concurrent schedule (the coarse cells away from the refinement block
-  // updated beside the fine updates and the transfer): a low-priority side stream and its
+  // updated beside the fine updates and the transfer): a lowest-priority side stream for
+  // those cells, a highest-priority stream for the fine updates and the transfer, and their
   // events, created on first use, or null
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev_near = nullptr, ev_far = nullptr;
+  cudaStream_t side = nullptr, hi = nullptr;
+  cudaEvent_t ev_near = nullptr, ev_far = nullptr, ev_hi = nullptr;
 };
 
 // Marks the held nu_t of the learned closure as out of date, so that the next update

@@ -933,13 +933,24 @@ __global__ void __launch_bounds__(256) force_partial_kernel(GridView<S> g, const
     for (int c = 0; c < 3; ++c) partial[blockIdx.x * 3 + c] = red[c][0];
 }
 
+// The partial sums added in block order by one thread (deterministic); every thread of the
+// block first stages a chunk of them in shared memory, so the serial sum waits on shared
+// memory instead of one global load after another.  One block, any number of threads.
 static __global__ void force_final_kernel(const double* partial, int nblocks, double* out) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    double s[3] = {0, 0, 0};
-    for (int b = 0; b < nblocks; ++b)
-      for (int c = 0; c < 3; ++c) s[c] += partial[b * 3 + c];
-    for (int c = 0; c < 3; ++c) out[c] = s[c];
+  constexpr int kChunk = 512;  // blocks per staged chunk (12 KB)
+  __shared__ double stage[kChunk * 3];
+  double s[3] = {0, 0, 0};
+  for (int b0 = 0; b0 < nblocks; b0 += kChunk) {
+    const int nb = min(kChunk, nblocks - b0);
+    for (int i = threadIdx.x; i < nb * 3; i += blockDim.x) stage[i] = partial[b0 * 3 + i];
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int b = 0; b < nb; ++b)
+        for (int c = 0; c < 3; ++c) s[c] += stage[b * 3 + c];
+    __syncthreads();
   }
+  if (threadIdx.x == 0 && blockIdx.x == 0)
+    for (int c = 0; c < 3; ++c) out[c] = s[c];
 }
 
 // ------------------------------------------------------------------------------------------

@@ -120,7 +120,7 @@ int psl_momentum_exchange_force_noalloc(const float* populations, long long row_
   force_partial_kernel<StoreF32><<<nb, kNoAllocThreads, 0, stream>>>(
       g, markers, nx, ny, box_lo3[0], box_lo3[1], box_lo3[2], box_hi3[0] - box_lo3[0], box_hi3[1] - box_lo3[1],
       box_hi3[2] - box_lo3[2], scratch);
-  force_final_kernel<<<1, 32, 0, stream>>>(scratch, nb, force3);
+  force_final_kernel<<<1, 256, 0, stream>>>(scratch, nb, force3);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     return noalloc_fail(PSL_ERR_CUDA, std::string("psl_momentum_exchange_force_noalloc: ") + cudaGetErrorString(e));

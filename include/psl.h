@@ -160,7 +160,9 @@ int psl_apply_local_cell_update(psl_grid* grid);
 /* applyBCPeriodicX / applyBCPeriodicY (boundaryConditions/periodicXY.h:11,57). */
 int psl_apply_bc_periodic_x(psl_grid* grid);
 int psl_apply_bc_periodic_y(psl_grid* grid);
-/* applyCoarseFineGridCommunication (gridRefinementFunctions.h:433-526): one kernel. */
+/* applyCoarseFineGridCommunication (gridRefinementFunctions.h:433-526): one kernel, launched
+ * twice in stream order on the coarse grid's stream (restriction onto the coarse ring, then
+ * prolongation into the fine shell). */
 int psl_apply_coarse_fine_grid_communication(psl_grid* coarse, psl_grid* fine);
 /* fillCoarseGridFromFine (gridRefinementFunctions.h:528-535): every coarse cell of
  * [iS+1, iE-1) x [jS+1, jE-1) x [kS+1, kE-1) (inside the refinement block) becomes the

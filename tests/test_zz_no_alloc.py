@@ -156,3 +156,55 @@ def test_noalloc_force_in_a_captured_graph_and_after_a_larger_box():
     del graph
     for gr in grids:
         gr.close()
+
+
+def test_noalloc_force_over_more_blocks_than_one_staged_chunk():
+    """A box of more than 512 x 4096 cells: the final sum then stages the partial sums in
+    two chunks of shared memory.  The sphere sits against the top of the grid, so solid
+    cells fall into blocks of the second chunk; the whole grid's force equals the force over
+    the sphere's own box (one chunk), since only solid cells contribute."""
+    import torch
+
+    from periodicshiftlbm_b200 import _lib, updateGrid
+    from periodicshiftlbm_b200.cases import SphereConfig, make_sphere_grids
+
+    cfg = SphereConfig(name="noalloc_big", nx=132, ny=128, nz=128, sphere=(60.0, 64.0, 121.5), radius=6.0,
+                       u_in=0.05, nu=0.01, smagorinsky=0.1)
+    grids, case = make_sphere_grids(cfg)
+    g = grids[0]
+    info = g.Info
+    n = info.cellCount
+    assert n > 512 * 4096
+    for _ in range(3):
+        updateGrid(grids, 0)
+    lo, hi = _box(case, info)
+    whole_lo = np.zeros(3, dtype=np.int32)
+    whole_hi = np.array([info.cellCountX, info.cellCountY, info.cellCountZ], dtype=np.int32)
+    markers_host = g.markers
+    solid = (markers_host.reshape(-1) & 7) == 2
+    ks = np.nonzero(solid)[0] // (info.cellCountX * info.cellCountY)
+    assert ks.max() >= 125  # solid cells in blocks 512 and above of the whole-grid box
+    L = _lib.lib()
+    shifts = g.shifter.astype(np.int32)
+    rows = torch.from_numpy(_rows_with_shifts(g.fArray, shifts, n)).cuda()
+    markers = torch.from_numpy(markers_host).cuda()
+    whole = torch.full((3,), float("nan"), dtype=torch.float64, device="cuda")
+    box = torch.full((3,), float("nan"), dtype=torch.float64, device="cuda")
+    s = torch.cuda.Stream()
+
+    def call(box_lo, box_hi, dst):
+        return L.psl_momentum_exchange_force_noalloc(
+            ctypes.c_void_p(rows.data_ptr()), n, shifts.ctypes.data, n, ctypes.c_void_p(markers.data_ptr()),
+            info.cellCountX, info.cellCountY, info.cellCountZ, box_lo.ctypes.data, box_hi.ctypes.data,
+            ctypes.c_void_p(dst.data_ptr()), ctypes.c_void_p(s.cuda_stream))
+
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        assert call(whole_lo, whole_hi, whole) == 0, L.psl_last_error()
+        assert call(lo, hi, box) == 0, L.psl_last_error()
+    torch.cuda.synchronize()
+    w, b = whole.cpu().numpy(), box.cpu().numpy()
+    assert np.all(np.isfinite(w)) and abs(b).max() > 0
+    assert np.allclose(w, b, rtol=TOL, atol=TOL * np.abs(b).max()), (w, b)
+    for gr in grids:
+        gr.close()

@@ -704,10 +704,15 @@ static int launch_coarse_fine(psl_grid* c, psl_grid* f) {
   p.n_ring = (uint32_t)(ra * rb * rc - (ra - 2) * (rb - 2) * (rc - 2));
   // z faces, y faces, then four lanes per x-row boundary (coarse_fine_kernel)
   p.n_shell = (uint32_t)(4LL * p.fnx * p.fny + 4LL * p.fnx * (p.fnz - 4) + 4LL * (p.fny - 3) * (p.fnz - 4));
-  coarse_fine_kernel<S, 1><<<std::max(1u, blocks_for(p.n_ring, kCoarseFineThreads)), kCoarseFineThreads, 0,
-                             c->stream>>>(p);
-  coarse_fine_kernel<S, 2><<<std::max(1u, blocks_for(p.n_shell, kCoarseFineThreads)), kCoarseFineThreads, 0,
-                             c->stream>>>(p);
+  const unsigned int ring_blocks = std::max(1u, blocks_for(p.n_ring, kCoarseFineThreads));
+  const unsigned int shell_blocks = std::max(1u, blocks_for(p.n_shell, kCoarseFineThreads));
+  if (c->f_twice && f->f_twice) {  // both grids' rows mapped twice: no wrap test
+    coarse_fine_kernel<S, 1, true><<<ring_blocks, kCoarseFineThreads, 0, c->stream>>>(p);
+    coarse_fine_kernel<S, 2, true><<<shell_blocks, kCoarseFineThreads, 0, c->stream>>>(p);
+  } else {
+    coarse_fine_kernel<S, 1, false><<<ring_blocks, kCoarseFineThreads, 0, c->stream>>>(p);
+    coarse_fine_kernel<S, 2, false><<<shell_blocks, kCoarseFineThreads, 0, c->stream>>>(p);
+  }
   PSL_CUDA(cudaGetLastError());
   return PSL_OK;
 }

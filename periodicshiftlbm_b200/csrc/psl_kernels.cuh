@@ -701,13 +701,16 @@ constexpr uint32_t kAllDirs = (1u << 27) - 1;
 // The prolongation's coarse reads use ordinary (L1-cached) loads: it is a launch of its own
 // after the restriction's, and L1 starts empty for every launch, so no stale copy of a
 // restricted ring cell can be hit.
-template <typename S>
+// kFlat: the grid's rows are mapped twice (rows 2N apart), so cell + off_q needs no wrap.
+template <bool kFlat = false, typename S>
 __device__ __forceinline__ typename S::calc load_pop(const RowIndex<S>& r, int q, uint32_t cell) {
-  return S::load_q(r.base + (cell + r.off[q] - (cell >= r.lim[q] ? r.n : 0u)), q);
+  if constexpr (kFlat) return S::load_q(r.base + (cell + r.off[q]), q);
+  else return S::load_q(r.base + (cell + r.off[q] - (cell >= r.lim[q] ? r.n : 0u)), q);
 }
-template <typename S>
+template <bool kFlat = false, typename S>
 __device__ __forceinline__ void store_pop(const RowIndex<S>& r, int q, uint32_t cell, typename S::calc v) {
-  S::store_q(r.base + (cell + r.off[q] - (cell >= r.lim[q] ? r.n : 0u)), v, q);
+  if constexpr (kFlat) S::store_q(r.base + (cell + r.off[q]), v, q);
+  else S::store_q(r.base + (cell + r.off[q] - (cell >= r.lim[q] ? r.n : 0u)), v, q);
 }
 
 // Work items are dealt out in warp-sized chunks, consecutive chunks to consecutive blocks,
@@ -722,7 +725,7 @@ constexpr int kCoarseFineThreads = 128;
 // Coarse cell (i, j, k) of the refined block from its 8 fine children: their populations
 // added in the child order (k, j, i outer to inner), averaged, rescaled fine -> coarse
 // (writeToCoarseGridInterface, gridRefinementFunctions.h:283-336).
-template <typename S>
+template <bool kFlat = false, typename S>
 __device__ __forceinline__ void restrict_cell(const RowIndex<S>& rc, const RowIndex<S>& rf, const CoarseFineParams<S>& p,
                                               int i, int j, int k) {
   using T = typename S::calc;
@@ -738,13 +741,13 @@ __device__ __forceinline__ void restrict_cell(const RowIndex<S>& rc, const RowIn
   for (int q = 0; q < 27; ++q) {
     T v = T(0);
 #pragma unroll
-    for (int c = 0; c < 8; ++c) v = rn_add(v, load_pop(rf, q, fc[c]));
+    for (int c = 0; c < 8; ++c) v = rn_add(v, load_pop<kFlat>(rf, q, fc[c]));
     f[q] = v * T(0.125);
   }
   rescale(f, false);
   const uint32_t cc = ((uint32_t)k * p.cny + j) * p.cnx + i;
 #pragma unroll
-  for (int q = 0; q < 27; ++q) store_pop(rc, q, cc, f[q]);
+  for (int q = 0; q < 27; ++q) store_pop<kFlat>(rc, q, cc, f[q]);
 }
 
 // fillCoarseGridFromFine (gridRefinementFunctions.h:528-535): every coarse cell of the box
@@ -761,7 +764,8 @@ __global__ void __launch_bounds__(kCoarseFineThreads) fill_coarse_kernel(const _
 // kPhase 1: the restriction, 2: the prolongation, as two ordinary launches in stream order
 // (the launch boundary orders them; one cooperative launch with a grid barrier between the
 // phases ran 0.174 / 0.167 ms per FP32 / FP16 transfer against 0.168 / 0.154 for the two).
-template <typename S, int kPhase>
+// kFlat: both grids' rows are mapped twice (no wrap test on any population address).
+template <typename S, int kPhase, bool kFlat>
 __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const __grid_constant__ CoarseFineParams<S> p) {
   using T = typename S::calc;
   // The row offsets of both grids are read from shared memory inside the item loops (kept
@@ -805,7 +809,7 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
         rj = 1 + r % (b - 2);
         rk = 1 + r / (b - 2);
       }
-      restrict_cell(rc, rf, p, p.iS + 1 + ri, p.jS + 1 + rj, p.kS + 1 + rk);
+      restrict_cell<kFlat>(rc, rf, p, p.iS + 1 + ri, p.jS + 1 + rj, p.kS + 1 + rk);
     }
   }
   if (kPhase == 1) return;
@@ -877,15 +881,15 @@ __global__ void __launch_bounds__(kCoarseFineThreads) coarse_fine_kernel(const _
     T f[27];
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
-      T v = load_pop(rc, q, pc);
+      T v = load_pop<kFlat>(rc, q, pc);
 #pragma unroll
-      for (int t = 0; t < 6; ++t) v = rn_add(v, load_pop(rc, q, nc[t]) * w[t]);
+      for (int t = 0; t < 6; ++t) v = rn_add(v, load_pop<kFlat>(rc, q, nc[t]) * w[t]);
       f[q] = v;
     }
     rescale(f, true);
 #pragma unroll
     for (int q = 0; q < 27; ++q)
-      if (mask & (1u << q)) store_pop(rf, q, fcell, f[q]);
+      if (mask & (1u << q)) store_pop<kFlat>(rf, q, fcell, f[q]);
   }
 }
 
